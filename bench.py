@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the SPEEDY column physics on B200.
+
+Metric: physics columns/s (higher is better).  One step = one physics-tendency pass over the
+workload's columns with inputs resident in HBM.  Default workload: the ragged ensemble
+(32xT21, 16xT31, 8xT42, 4xT85, 1xT170 = 466,944 columns, half-ish at 16 levels), seeded
+synthetic fields.  Inputs plus outputs of one step (~200 MB) exceed the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload ensemble|t425|t31] [--mode batched|plain]
+
+Under torchrun each rank runs its own copy of the workload (weak scaling, no collective on the
+data path); the timing is the max over ranks.  ``--impl reference`` times the CPU port of the
+reference physics (the oracle) on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# DRAM bytes (read + write) per column of the fused forward, from the committed ncu summaries
+# (profiles/); None until a capture exists for the workload.
+NCU_TRAFFIC_PER_COLUMN = {}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "t425", "t31"])
+    ap.add_argument("--mode", default="plain", choices=["batched", "plain"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_members(pkg, name, rank=0):
+    syn = pkg.synthetic
+    if name == "ensemble":
+        return syn.ensemble_members(base_seed=1000 + 1000 * rank)
+    if name == "t425":
+        return [syn.t425_instance(seed=425 + rank)]
+    return [syn.config0_instance(seed=rank, lfluxland=True)]
+
+
+def workload_config(name, members, mode):
+    cols = sum(m.columns for m in members)
+    c8 = sum(m.columns for m in members if m.kx == 8)
+    desc = {"ensemble": "ragged ensemble 32xT21+16xT31+8xT42+4xT85+1xT170, 8/16 levels",
+            "t425": "T425 1280x640, 16 levels", "t31": "T31 96x48 aquaplanet, 8 levels"}[name]
+    return {"workload": desc, "members": len(members), "columns": cols, "columns_kx8": c8,
+            "columns_kx16": cols - c8, "mode": mode,
+            "l2": "inputs+outputs per step exceed the 126 MB L2" if cols > 100000 else
+                  "L2 flushed between steps"}
+
+
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while it runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_b200(args):
+    import torch
+    pkg = importlib.import_module("jax-gcm_b200")
+    from tests.helpers import to_device
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    members = workload_members(pkg, args.workload, rank)
+    cols = sum(m.columns for m in members)
+    bytes_step = sum(pkg.synthetic.fwd_bytes(m.kx, m.columns) for m in members)
+
+    # device-resident inputs and preallocated outputs
+    runs = []
+    for m in members:
+        state, forcing, geom, date = to_device(pkg, m, dev)
+        phys = pkg.SpeedyPhysics(diagnostics=False)
+        e3 = lambda: torch.empty((m.kx, m.ix, m.il), dtype=torch.float32, device=dev)
+        e2 = lambda: torch.empty((m.ix, m.il), dtype=torch.float32, device=dev)
+        out = dict(u_wind=e3(), v_wind=e3(), temperature=e3(), specific_humidity=e3(),
+                   precnv=e2(), precls=e2())
+        runs.append((m, state, forcing, geom, date, phys, out))
+
+    def step():
+        for (_, state, forcing, geom, date, phys, out) in runs:
+            phys.compute_tendencies(state, forcing, geom, date, out=out)
+
+    launches_per_step = 2 * len(runs)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    time.sleep(0.3)
+    total_ms = timed(step, args.steps, args.warmup)
+    clk = clocks.stop()
+    ms_step = total_ms / args.steps
+    value = cols * world / (ms_step / 1e3)
+
+    # roofline of the fused forward (cloud-top pre-pass + column kernel), per launch pair
+    peak, peak_kind = load_peaks()
+    achieved = bytes_step / (ms_step / 1e3) / 1e9
+    traffic = NCU_TRAFFIC_PER_COLUMN.get(args.workload)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "kernel": "cloudtop_prepass + column_kernel (one forward)",
+                "algorithmic_bytes_per_step": bytes_step,
+                "traffic": (traffic * cols if traffic else None)}
+
+    # end to end through the public API with host buffers (pinned), H2D + D2H timed
+    e2e = None
+    if not args.no_e2e:
+        host = []
+        h2d = d2h = 0
+        for (m, state, forcing, geom, date, phys, out) in runs:
+            hs = {}
+            for name, t in [("u", state.u_wind), ("v", state.v_wind), ("t", state.temperature),
+                            ("q", state.specific_humidity), ("phi", state.geopotential),
+                            ("psa", state.normalized_surface_pressure)]:
+                hs[name] = torch.empty(t.shape, dtype=t.dtype, pin_memory=True).copy_(t.cpu())
+                h2d += t.numel() * 4
+            ho = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                  for k, v in out.items() if k in ("temperature", "specific_humidity",
+                                                   "u_wind", "v_wind", "precnv", "precls")}
+            d2h += sum(v.numel() * 4 for v in ho.values())
+            host.append((hs, ho))
+
+        def e2e_step():
+            for (hs, ho), (m, state, forcing, geom, date, phys, out) in zip(host, runs):
+                state.u_wind.copy_(hs["u"], non_blocking=True)
+                state.v_wind.copy_(hs["v"], non_blocking=True)
+                state.temperature.copy_(hs["t"], non_blocking=True)
+                state.specific_humidity.copy_(hs["q"], non_blocking=True)
+                state.geopotential.copy_(hs["phi"], non_blocking=True)
+                state.normalized_surface_pressure.copy_(hs["psa"], non_blocking=True)
+                phys.compute_tendencies(state, forcing, geom, date, out=out)
+                for k, v in ho.items():
+                    v.copy_(out[k], non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+
+        e2e_ms = timed(e2e_step, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
+        e2e = {"value": cols * world / (e2e_ms / 1e3), "unit": "columns/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": round(e2e_ms, 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(members)
+
+    if rank == 0:
+        line = {"metric": "physics columns/s", "value": round(value, 1), "unit": "columns/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generators with the workload's shapes and distributions)",
+                "config": workload_config(args.workload, members, args.mode),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "gpu_launches": launches_per_step * args.steps}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+_MEMBER_CACHE = {}
+
+
+def _oracle_member(args):
+    """Runs the oracle on one member in a worker process (inputs generated once per worker)."""
+    import importlib as il
+    from oracle import speedy_oracle as O
+    if args not in _MEMBER_CACHE:
+        pkg = il.import_module("jax-gcm_b200")
+        kind, seed, ix, il_, kx = args
+        inst = pkg.synthetic.land_instance(seed, ix, il_, kx)
+        _MEMBER_CACHE[args] = (inst.columns, inst.oracle_args(O.default_parameters()))
+    cols, oargs = _MEMBER_CACHE[args]
+    t0 = time.perf_counter()
+    O.compute_tendencies(*oargs)
+    return cols, time.perf_counter() - t0
+
+
+def cpu_baseline(members, repeats=2):
+    """The oracle (NumPy port of the reference physics) on one host core over the whole
+    workload, repeated; columns/s."""
+    from oracle import speedy_oracle as O
+    done, secs = 0, 0.0
+    for _ in range(repeats):
+        for m in members:
+            args = m.oracle_args(O.default_parameters())
+            t0 = time.perf_counter()
+            O.compute_tendencies(*args)
+            secs += time.perf_counter() - t0
+            done += m.columns
+    return {"value": round(done / secs, 1), "unit": "columns/s", "cores": 1, "kind": "port",
+            "sample": f"{repeats} passes of the NumPy oracle over all {len(members)} members "
+                      f"({sum(m.columns for m in members)} columns), one core"}
+
+
+def run_reference(args):
+    """The reference arm: the CPU port of the reference physics on all host cores."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    pkg = importlib.import_module("jax-gcm_b200")
+    members = workload_members(pkg, args.workload, 0)
+    jobs = []
+    for n, m in enumerate(members):
+        jobs.append(("land", 1000 + n, m.ix, m.il, m.kx))
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    cols = sum(m.columns for m in members)
+    with ctx.Pool(cores) as pool:
+        for _ in range(max(1, args.warmup)):
+            pool.map(_oracle_member, jobs, chunksize=1)
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            res = pool.map(_oracle_member, jobs, chunksize=1)
+            done += sum(r[0] for r in res)
+        el = time.perf_counter() - t0
+    value = done / el
+    line = {"impl": "reference", "metric": "physics columns/s", "value": round(value, 1),
+            "unit": "columns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators with the workload's shapes and distributions)",
+            "config": workload_config(args.workload, members, "reference"),
+            "cpu_baseline": {"value": round(value, 1), "unit": "columns/s", "cores": cores,
+                             "kind": "port",
+                             "sample": f"each step: the NumPy port of the reference physics over "
+                                       f"all {len(members)} members ({cols} columns) spread "
+                                       f"over {cores} worker processes (inputs pre-generated)"},
+            "e2e": {"value": round(value, 1), "unit": "columns/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

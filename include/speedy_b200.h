@@ -1,0 +1,143 @@
+/*
+ * speedy_b200.h -- C ABI of the B200 (sm_100a) SPEEDY column physics.
+ *
+ * The entry points replace the reference's SPEEDY physics call
+ *   SpeedyPhysics.compute_tendencies(state, forcing, geometry, date)
+ *     (jcm/physics/speedy/speedy_physics.py:88-127)
+ * as it is invoked from
+ *   get_physical_tendencies (jcm/physics_interface.py:344-383),
+ * including the verify_state / verify_tendencies clamps around it
+ *   (jcm/physics_interface.py:305-342, fused behind SPD_FUSE_VERIFY).
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers owned by the caller; the library never frees them.
+ *  - Layout is the reference's: level fields are [kx][ix][il] row-major (column c = i*il + j,
+ *    latitude index j = c % il), surface fields [ix][il], latitude tables [il] south->north.
+ *  - float32 everywhere (the reference computes in float32).
+ *  - Every call is asynchronous on `stream` (a cudaStream_t passed as void*), makes no host
+ *    synchronisation and allocates no memory; scratch is caller-provided.
+ *  - Return value 0 (SPD_OK) or one of the SPD_ERR_* codes; no exceptions cross the ABI.
+ */
+#ifndef SPEEDY_B200_H
+#define SPEEDY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPD_MAX_KX 16
+#define SPD_ABI_VERSION 1
+
+enum spd_status {
+  SPD_OK = 0,
+  SPD_ERR_NULL = 1,      /* a required pointer is NULL */
+  SPD_ERR_SHAPE = 2,     /* ix, il, member count or column count out of range */
+  SPD_ERR_KX = 3,        /* unsupported level count (supported: 7, 8, 16) */
+  SPD_ERR_SCRATCH = 4,   /* scratch buffer NULL, too small or not 256-byte aligned */
+  SPD_ERR_CUDA = 5,      /* a CUDA launch or runtime call failed */
+  SPD_ERR_DEVICE = 6,    /* the device reported an error status (bounded wait expired, ...) */
+  SPD_ERR_ALIGN = 7      /* a field pointer is not 16-byte aligned */
+};
+
+/* spd_desc_t.flags */
+enum spd_flags {
+  SPD_LFLUXLAND = 1u << 0,    /* ForcingData.lfluxland (jcm/forcing.py:17) */
+  SPD_LSCASYM = 1u << 1,      /* SurfaceFluxParameters.lscasym (params.py:180) */
+  SPD_LSKINEB = 1u << 2,      /* SurfaceFluxParameters.lskineb (params.py:181) */
+  SPD_INCREASE_CO2 = 1u << 3, /* ForcingParameters.increase_co2 (params.py:34) */
+  SPD_FUSE_VERIFY = 1u << 4   /* apply verify_state before and verify_tendencies after */
+};
+
+/* One grid instance: shape, switches and DateData (jcm/date.py:9-14). */
+typedef struct {
+  int32_t kx, ix, il;
+  uint32_t flags;
+  float tyear;          /* DateData.tyear */
+  int32_t model_year;   /* DateData.model_year */
+  int32_t model_step;   /* DateData.model_step: shortwave heating when model_step % 3 == 0 */
+  int32_t co2_year_ref; /* ForcingParameters.co2_year_ref */
+  float dt_seconds;     /* time step of the fused verify_tendencies limiter */
+  float q_tend_scale;   /* factor applied to the humidity tendency last (1 = g/kg/s) */
+} spd_desc_t;
+
+/* Vertical sigma tables of Geometry (jcm/geometry.py:62-85, :99-106), by value. */
+typedef struct {
+  float hsg[SPD_MAX_KX + 1];
+  float fsg[SPD_MAX_KX];
+  float dhs[SPD_MAX_KX];
+  float sigl[SPD_MAX_KX];
+  float grdsig[SPD_MAX_KX];
+  float grdscp[SPD_MAX_KX];
+  float wvi[SPD_MAX_KX][2];
+} spd_vgrid_t;
+
+/* The float leaves of Parameters (jcm/physics/speedy/params.py:9-232), by value. */
+typedef struct {
+  /* ConvectionParameters */
+  float psmin, trcnv, rhil, rhbl, entmax, smf;
+  /* CondensationParameters */
+  float trlsc, rhlsc, drhlsc, rhblsc;
+  /* ShortwaveRadiationParameters */
+  float albcl, albcls, absdry, absaer, abswv1, abswv2, abscl1, abscl2;
+  float ablwin, ablwv1, ablwv2, ablcl1, ablcl2;
+  float rhcl1, rhcl2, qacl, wpcl, pmaxcl, clsmax, clsminl, gse_s0, gse_s1;
+  /* ModRadConParameters */
+  float albsea, albice, albsn, epslw, emisfc;
+  /* SurfaceFluxParameters */
+  float fwind0, ftemp0, fhum0, cdl, cds, chl, chs, vgust, ctday, dtheta, fstab;
+  float clambda, clambsn, hdrag;
+  /* VerticalDiffusionParameters */
+  float trshc, trvdi, trvds, redshc, rhgrad, segrad;
+} spd_params_t;
+
+/* PhysicsState (physics_interface.py:22-29), ForcingData day slice (jcm/forcing.py:8-17)
+ * and the per-column / per-latitude Geometry fields (jcm/geometry.py:91-97). */
+typedef struct {
+  const float *u_wind, *v_wind, *temperature, *specific_humidity, *geopotential; /* [kx][C] */
+  const float *normalized_surface_pressure;                                        /* [C] */
+  const float *alb0, *sice_am, *snowc_am, *soilw_am, *stl_am, *sea_surface_temperature;
+  const float *fmask, *orog, *phis0;                                               /* [C] */
+  const float *sia, *coa;                                                          /* [il] */
+} spd_inputs_t;
+
+/* PhysicsTendency (physics_interface.py:89-94) plus the PhysicsData leaves the kernel fills.
+ * Tendency planes and precnv/precls are required; every other pointer may be NULL. */
+typedef struct {
+  float *u_wind, *v_wind, *temperature, *specific_humidity; /* [kx][C] */
+  float *precnv, *precls;                                    /* [C] */
+  float *cbmf, *cloudc, *cloudstr, *rsds, *rsns, *ftop_sw;   /* [C], nullable */
+  float *rlds, *rlns, *ftop_lw, *tsfc, *tskin, *shf, *evap;  /* [C], nullable */
+  int32_t *iptop, *icltop;                                   /* [C], nullable */
+} spd_outputs_t;
+
+/* ----------------------------------------------------------------------------------------- */
+/* Plain drop-in: one instance per call.                                                      */
+/* ----------------------------------------------------------------------------------------- */
+
+/* Scratch bytes spd_fwd needs for this descriptor (per-instance cloud-top level set, the
+ * per-latitude solar tables and a status word). */
+size_t spd_fwd_scratch_bytes(const spd_desc_t* desc);
+
+/* SpeedyPhysics.compute_tendencies for one instance (speedy_physics.py:88-127).
+ * Two launches on `stream`: a cloud-top pre-pass that forms the instance's level set
+ * (shortwave_radiation.py:62-68) and the fused column kernel.  `scratch` must be 256-byte
+ * aligned and at least spd_fwd_scratch_bytes(desc) long; it is initialised by the call. */
+int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+            const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
+            size_t scratch_bytes, void* stream);
+
+/* ----------------------------------------------------------------------------------------- */
+/* Helpers                                                                                    */
+/* ----------------------------------------------------------------------------------------- */
+const char* spd_status_string(int status);
+int spd_abi_version(void);
+/* Fills `params` with Parameters.default() (params.py:244-254). */
+void spd_default_params(spd_params_t* params);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPEEDY_B200_H */

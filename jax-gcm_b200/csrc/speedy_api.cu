@@ -1,0 +1,262 @@
+// speedy_api.cu -- kernels and C-ABI entry points of the plain per-instance drop-in.
+//
+// spd_fwd runs two launches on the caller's stream:
+//   1. cloudtop_prepass: every column forms its cloud-top level clip(icltop, 0, kx-1) and the
+//      instance ORs them into one 32-bit level set S (the cross-column dependency of
+//      shortwave_radiation.py:62-68); the same launch writes the per-latitude solar table.
+//   2. column_kernel: the fused physics of every column (speedy_physics.py:88-127), reading S.
+// One thread owns one column; the per-level fields live in registers.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "speedy_column.cuh"
+
+namespace spd {
+
+constexpr int kBlock = 128;
+constexpr size_t kHeaderBytes = 256;  // S word, status word, padding
+
+template <int KX>
+__device__ __forceinline__ void load_levels(const float* __restrict__ f, int C, int c, float v[KX]) {
+#pragma unroll
+  for (int k = 0; k < KX; ++k) v[k] = __ldg(f + (size_t)k * C + c);
+}
+
+// Level set of one block, OR-ed into the instance word once per block.
+__device__ __forceinline__ void or_level_set(uint32_t bit, uint32_t* S) {
+  __shared__ uint32_t warp_bits[kBlock / 32];
+  bit = __reduce_or_sync(0xffffffffu, bit);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_bits[warp] = bit;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t b = 0;
+#pragma unroll
+    for (int w = 0; w < kBlock / 32; ++w) b |= warp_bits[w];
+    const uint32_t have = *reinterpret_cast<volatile uint32_t*>(S);
+    if ((have & b) != b) atomicOr(S, b);
+  }
+}
+
+template <int KX>
+__global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const spd_inputs_t in,
+                                                           uint32_t* __restrict__ S,
+                                                           ZonalRow* __restrict__ table) {
+  const int c = blockIdx.x * kBlock + threadIdx.x;
+  if (c < K.il) table[c] = zonal_row(K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
+  uint32_t bit = 0;
+  if (c < K.C) {
+    float t[KX], q[KX], phi[KX];
+    load_levels<KX>(in.temperature, K.C, c, t);
+    load_levels<KX>(in.specific_humidity, K.C, c, q);
+    load_levels<KX>(in.geopotential, K.C, c, phi);
+    if (K.flags & SPD_FUSE_VERIFY) {
+#pragma unroll
+      for (int k = 0; k < KX; ++k) q[k] = (q[k] < 0.0f) ? 0.0f : q[k];
+    }
+    const float psa = __ldg(in.normalized_surface_pressure + c);
+    const int icl = column_icltop<KX>(K, t, q, phi, psa);
+    bit = 1u << min(max(icl, 0), KX - 1);
+  }
+  or_level_set(bit, S);
+}
+
+template <int KX>
+__global__ void __launch_bounds__(kBlock) column_kernel(const Consts K, const spd_inputs_t in,
+                                                        const spd_outputs_t out,
+                                                        const uint32_t* __restrict__ S,
+                                                        const ZonalRow* __restrict__ table) {
+  const int c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= K.C) return;
+  const int C = K.C;
+  float t[KX], q[KX], phi[KX];
+  load_levels<KX>(in.temperature, C, c, t);
+  load_levels<KX>(in.specific_humidity, C, c, q);
+  load_levels<KX>(in.geopotential, C, c, phi);
+  SurfaceIn s;
+  s.psa = __ldg(in.normalized_surface_pressure + c);
+  s.u_low = __ldg(in.u_wind + (size_t)(KX - 1) * C + c);
+  s.v_low = __ldg(in.v_wind + (size_t)(KX - 1) * C + c);
+  s.sst = __ldg(in.sea_surface_temperature + c);
+  s.stl = __ldg(in.stl_am + c);
+  s.soilw = __ldg(in.soilw_am + c);
+  s.snowc = __ldg(in.snowc_am + c);
+  s.sice = __ldg(in.sice_am + c);
+  s.alb0 = __ldg(in.alb0 + c);
+  s.fmask = __ldg(in.fmask + c);
+  s.orog = __ldg(in.orog + c);
+  s.phis0 = __ldg(in.phis0 + c);
+  const ZonalRow z = table[c % K.il];
+  const uint32_t Sw = __ldg(S);
+  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
+  uint32_t neg = 0;
+  if (verify) {
+#pragma unroll
+    for (int k = 0; k < KX; ++k) {
+      if (q[k] < 0.0f) {
+        neg |= 1u << k;
+        q[k] = 0.0f;
+      }
+    }
+  }
+  ColumnOut<KX> o;
+  column_full<KX>(K, t, q, phi, s, z, Sw, o);
+  // verify_tendencies (physics_interface.py:321-342) with the unclamped humidity
+  if (verify) {
+    const float dt = K.dt_seconds;
+#pragma unroll
+    for (int k = 0; k < KX; ++k) {
+      const float qr = (neg >> k & 1u) ? __ldg(in.specific_humidity + (size_t)k * C + c) : q[k];
+      o.dq[k] = (qr + dt * o.dq[k] >= 0.0f) ? o.dq[k] : -qr / dt;
+    }
+  }
+  if (K.q_tend_scale != 1.0f) {
+#pragma unroll
+    for (int k = 0; k < KX; ++k) o.dq[k] = o.dq[k] * K.q_tend_scale;
+  }
+#pragma unroll
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    __stcs(out.u_wind + i, k == KX - 1 ? o.du_low : 0.0f);
+    __stcs(out.v_wind + i, k == KX - 1 ? o.dv_low : 0.0f);
+    __stcs(out.temperature + i, o.dt[k]);
+    __stcs(out.specific_humidity + i, o.dq[k]);
+  }
+  __stcs(out.precnv + c, o.precnv);
+  __stcs(out.precls + c, o.precls);
+  if (out.cbmf) out.cbmf[c] = o.cbmf;
+  if (out.cloudc) out.cloudc[c] = o.cloudc;
+  if (out.cloudstr) out.cloudstr[c] = o.clstr;
+  if (out.rsds) out.rsds[c] = o.rsds;
+  if (out.rsns) out.rsns[c] = o.rsns;
+  if (out.ftop_sw) out.ftop_sw[c] = o.ftop_sw;
+  if (out.rlds) out.rlds[c] = o.rlds;
+  if (out.rlns) out.rlns[c] = o.rlns;
+  if (out.ftop_lw) out.ftop_lw[c] = o.ftop_lw;
+  if (out.tsfc) out.tsfc[c] = o.tsfc;
+  if (out.tskin) out.tskin[c] = o.tskin;
+  if (out.shf) out.shf[c] = o.shf;
+  if (out.evap) out.evap[c] = o.evap;
+  if (out.iptop) out.iptop[c] = o.iptop;
+  if (out.icltop) out.icltop[c] = o.icltop;
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out) {
+  if (!d || !in || !out) return SPD_ERR_NULL;
+  if (d->kx != 7 && d->kx != 8 && d->kx != 16) return SPD_ERR_KX;
+  if (d->ix <= 0 || d->il <= 0 || (int64_t)d->ix * d->il > (1 << 30)) return SPD_ERR_SHAPE;
+  const void* req[] = {in->u_wind, in->v_wind, in->temperature, in->specific_humidity,
+                       in->geopotential, in->normalized_surface_pressure, in->alb0, in->sice_am,
+                       in->snowc_am, in->soilw_am, in->stl_am, in->sea_surface_temperature,
+                       in->fmask, in->orog, in->phis0, in->sia, in->coa, out->u_wind,
+                       out->v_wind, out->temperature, out->specific_humidity, out->precnv,
+                       out->precls};
+  for (const void* p : req)
+    if (!p) return SPD_ERR_NULL;
+  for (const void* p : req)
+    if (!aligned16(p)) return SPD_ERR_ALIGN;
+  return SPD_OK;
+}
+
+Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p) {
+  Consts K;
+  K.vg = *vg;
+  K.p = *p;
+  K.C = d->ix * d->il;
+  K.il = d->il;
+  K.flags = d->flags;
+  K.tyear = d->tyear;
+  K.model_year = d->model_year;
+  K.model_step = d->model_step;
+  K.co2_year_ref = d->co2_year_ref;
+  K.dt_seconds = d->dt_seconds;
+  K.q_tend_scale = d->q_tend_scale;
+  return K;
+}
+
+template <int KX>
+static int launch_fwd(const Consts& K, const spd_inputs_t& in, const spd_outputs_t& out,
+                      uint32_t* S, ZonalRow* table, cudaStream_t st) {
+  const int grid = (K.C + kBlock - 1) / kBlock;
+  const int grid_a = (max(K.C, K.il) + kBlock - 1) / kBlock;
+  cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
+  column_kernel<KX><<<grid, kBlock, 0, st>>>(K, in, out, S, table);
+  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+}
+
+int dispatch_fwd(const Consts& K, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
+                 uint32_t* S, ZonalRow* table, cudaStream_t st) {
+  switch (kx) {
+    case 7: return launch_fwd<7>(K, in, out, S, table, st);
+    case 8: return launch_fwd<8>(K, in, out, S, table, st);
+    case 16: return launch_fwd<16>(K, in, out, S, table, st);
+    default: return SPD_ERR_KX;
+  }
+}
+
+}  // namespace spd
+
+extern "C" {
+
+size_t spd_fwd_scratch_bytes(const spd_desc_t* desc) {
+  if (!desc || desc->il <= 0) return 0;
+  const size_t table = (size_t)desc->il * sizeof(spd::ZonalRow);
+  return spd::kHeaderBytes + ((table + 255) / 256) * 256;
+}
+
+int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+            const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
+            size_t scratch_bytes, void* stream) {
+  int rc = spd::check_instance(desc, in, out);
+  if (rc != SPD_OK) return rc;
+  if (!vgrid || !params) return SPD_ERR_NULL;
+  if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) ||
+      scratch_bytes < spd_fwd_scratch_bytes(desc))
+    return SPD_ERR_SCRATCH;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const spd::Consts K = spd::make_consts(desc, vgrid, params);
+  uint32_t* S = static_cast<uint32_t*>(scratch);
+  spd::ZonalRow* table =
+      reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + spd::kHeaderBytes);
+  if (cudaMemsetAsync(S, 0, spd::kHeaderBytes, st) != cudaSuccess) return SPD_ERR_CUDA;
+  return spd::dispatch_fwd(K, desc->kx, *in, *out, S, table, st);
+}
+
+const char* spd_status_string(int status) {
+  switch (status) {
+    case SPD_OK: return "ok";
+    case SPD_ERR_NULL: return "a required pointer is NULL";
+    case SPD_ERR_SHAPE: return "shape out of range";
+    case SPD_ERR_KX: return "unsupported level count (supported: 7, 8, 16)";
+    case SPD_ERR_SCRATCH: return "scratch buffer NULL, too small or not 256-byte aligned";
+    case SPD_ERR_CUDA: return "CUDA launch or runtime call failed";
+    case SPD_ERR_DEVICE: return "device reported an error status";
+    case SPD_ERR_ALIGN: return "a field pointer is not 16-byte aligned";
+    default: return "unknown status";
+  }
+}
+
+int spd_abi_version(void) { return SPD_ABI_VERSION; }
+
+void spd_default_params(spd_params_t* p) {
+  if (!p) return;
+  *p = spd_params_t{};
+  p->psmin = 0.8f; p->trcnv = 6.0f; p->rhil = 0.7f; p->rhbl = 0.9f; p->entmax = 0.5f;
+  p->smf = 0.8f;
+  p->trlsc = 4.0f; p->rhlsc = 0.9f; p->drhlsc = 0.1f; p->rhblsc = 0.95f;
+  p->albcl = 0.43f; p->albcls = 0.50f; p->absdry = 0.033f; p->absaer = 0.033f;
+  p->abswv1 = 0.022f; p->abswv2 = 15.0f; p->abscl1 = 0.015f; p->abscl2 = 0.15f;
+  p->ablwin = 0.3f; p->ablwv1 = 0.7f; p->ablwv2 = 50.0f; p->ablcl1 = 12.0f; p->ablcl2 = 0.6f;
+  p->rhcl1 = 0.30f; p->rhcl2 = 1.0f; p->qacl = 0.20f; p->wpcl = 0.2f; p->pmaxcl = 10.0f;
+  p->clsmax = 0.60f; p->clsminl = 0.15f; p->gse_s0 = 0.25f; p->gse_s1 = 0.40f;
+  p->albsea = 0.07f; p->albice = 0.60f; p->albsn = 0.60f; p->epslw = 0.05f; p->emisfc = 0.98f;
+  p->fwind0 = 0.95f; p->ftemp0 = 1.0f; p->fhum0 = 0.0f; p->cdl = 2.4e-3f; p->cds = 1.0e-3f;
+  p->chl = 1.2e-3f; p->chs = 0.9e-3f; p->vgust = 5.0f; p->ctday = 1.0e-2f; p->dtheta = 3.0f;
+  p->fstab = 0.67f; p->clambda = 7.0f; p->clambsn = 7.0f; p->hdrag = 2000.0f;
+  p->trshc = 6.0f; p->trvdi = 24.0f; p->trvds = 6.0f; p->redshc = 0.5f; p->rhgrad = 0.5f;
+  p->segrad = 0.1f;
+}
+
+}  // extern "C"

@@ -150,10 +150,10 @@ def make_geometry(ix, il, kx, dtype=np.float32, lat="gaussian", orog=None, fmask
     geometry.py:128 leaves it unchanged.
     """
     hsg, fsg, dhs, sigl, grdsig, grdscp, wvi = vertical_tables(kx, dtype)
-    if lat == "gaussian":
+    if isinstance(lat, str) and lat == "gaussian":
         radang = gaussian_latitudes(il)
         sia, coa = np.sin(radang).astype(dtype), np.cos(radang).astype(dtype)
-    elif lat == "speedy":
+    elif isinstance(lat, str) and lat == "speedy":
         radang, sia, coa = speedy_latitudes(il)
         sia, coa = sia.astype(dtype), coa.astype(dtype)
     else:

@@ -1,0 +1,110 @@
+"""CPU checks of the C ABI: the library loads, exports every declared entry point, validates
+arguments before touching a GPU, and its parameter defaults agree with the reference's."""
+import ctypes as C
+import importlib
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    return importlib.import_module("jax-gcm_b200")
+
+
+@pytest.fixture(scope="module")
+def lib(pkg):
+    path = pkg._lib.LIB_PATH
+    if not os.path.exists(path):
+        import __graft_entry__
+        __graft_entry__.build()
+    return pkg._lib.load()
+
+
+def declared_functions():
+    names = []
+    for fn in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names += re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(spd_[a-z_0-9]+)\s*\(",
+                                text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "spd_fwd" in names and "spd_fwd_scratch_bytes" in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_abi_version(lib):
+    assert lib.spd_abi_version() == 1
+
+
+def test_default_params_match_reference_defaults(pkg, lib):
+    from oracle import speedy_oracle as O
+    p = pkg._lib.Params()
+    lib.spd_default_params(C.byref(p))
+    mine = pkg.Parameters.default().to_struct()
+    flat = {}
+    for g, d in O.PARAM_DEFAULTS.items():
+        flat.update(d)
+    for name in pkg._lib.PARAM_FIELDS:
+        assert getattr(p, name) == np.float32(flat[name]), name
+        assert getattr(mine, name) == np.float32(flat[name]), name
+
+
+def test_struct_sizes_match_header(pkg):
+    L = pkg._lib
+    assert C.sizeof(L.Desc) == 40
+    assert C.sizeof(L.VGrid) == 4 * (17 + 5 * 16 + 32)
+    assert C.sizeof(L.Params) == 4 * 57
+    assert C.sizeof(L.Inputs) == 8 * 17
+    assert C.sizeof(L.Outputs) == 8 * 21
+
+
+def test_scratch_bytes(pkg, lib):
+    d = pkg._lib.Desc(8, 96, 48, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    n = lib.spd_fwd_scratch_bytes(C.byref(d))
+    assert n >= 256 + 48 * 32 and n % 256 == 0
+
+
+def test_argument_validation_needs_no_gpu(pkg, lib):
+    L = pkg._lib
+    d = L.Desc(8, 96, 48, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    vg, pr, inp, out = L.VGrid(), L.Params(), L.Inputs(), L.Outputs()
+    rc = lib.spd_fwd(None, C.byref(vg), C.byref(pr), C.byref(inp), C.byref(out), None, 0, None)
+    assert rc == 1
+    rc = lib.spd_fwd(C.byref(d), C.byref(vg), C.byref(pr), C.byref(inp), C.byref(out), None, 0,
+                     None)
+    assert rc == 1  # null field pointers
+    d.kx = 9
+    rc = lib.spd_fwd(C.byref(d), C.byref(vg), C.byref(pr), C.byref(inp), C.byref(out), None, 0,
+                     None)
+    assert rc == 3
+    assert lib.spd_status_string(3).decode().startswith("unsupported")
+
+
+def test_product_path_fails_loudly_without_library(pkg, monkeypatch):
+    monkeypatch.setattr(pkg._lib, "_lib", None)
+    monkeypatch.setattr(pkg._lib, "LIB_PATH", "/nonexistent/libspeedy_b200.so")
+    with pytest.raises(pkg._lib.SpeedyLibraryError):
+        pkg._lib.load()
+
+
+def test_vertical_tables_match_oracle(pkg):
+    from oracle import speedy_oracle as O
+    for kx in (7, 8, 16):
+        a = pkg.physics.initialize_vertical(kx)
+        b = O.vertical_tables(kx)
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)

@@ -413,7 +413,8 @@ def test_speedy_single_column_smoke(params):
 
 
 def test_full_chain_finite_on_config0_like_state(params):
-    from oracle import synthetic
+    import importlib
+    synthetic = importlib.import_module("jax-gcm_b200").synthetic
     case = synthetic.config0_instance(seed=0, ix=32, il=16, lfluxland=True)
     tend, data = O.physics_step(*case.oracle_args(params))
     for f in (tend.u_wind, tend.v_wind, tend.temperature, tend.specific_humidity):
