@@ -8,7 +8,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = ["csrc/speedy_api.cu"]
-HEADERS = ["csrc/speedy_column.cuh", "../include/speedy_b200.h"]
+HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
+           "../include/speedy_b200.h"]
 OUT = os.path.join(HERE, "libspeedy_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

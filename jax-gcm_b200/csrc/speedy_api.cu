@@ -9,7 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "speedy_column.cuh"
+#include "speedy_column_smem.cuh"
 
 namespace spd {
 
@@ -62,17 +62,32 @@ __global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const
 }
 
 template <int KX>
-__global__ void __launch_bounds__(kBlock) column_kernel(const Consts K, const spd_inputs_t in,
+__global__ void __launch_bounds__(kNT, 2) column_kernel(const ConstsD CD, const spd_inputs_t in,
                                                         const spd_outputs_t out,
                                                         const uint32_t* __restrict__ S,
                                                         const ZonalRow* __restrict__ table) {
-  const int c = blockIdx.x * kBlock + threadIdx.x;
+  extern __shared__ float sm[];
+  const Consts& K = CD.K;
+  const int c = blockIdx.x * kNT + threadIdx.x;
   if (c >= K.C) return;
   const int C = K.C;
-  float t[KX], q[KX], phi[KX];
-  load_levels<KX>(in.temperature, C, c, t);
-  load_levels<KX>(in.specific_humidity, C, c, q);
-  load_levels<KX>(in.geopotential, C, c, phi);
+  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
+  float* tp = sm + (size_t)A_T * KX * kNT + threadIdx.x;
+  float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
+  float* pp = sm + (size_t)A_PHI * KX * kNT + threadIdx.x;
+  uint32_t neg = 0;
+#pragma unroll 4
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    tp[k * kNT] = __ldg(in.temperature + i);
+    float q = __ldg(in.specific_humidity + i);
+    if (verify && q < 0.0f) {
+      neg |= 1u << k;
+      q = 0.0f;
+    }
+    qp[k * kNT] = q;
+    pp[k * kNT] = __ldg(in.geopotential + i);
+  }
   SurfaceIn s;
   s.psa = __ldg(in.normalized_surface_pressure + c);
   s.u_low = __ldg(in.u_wind + (size_t)(KX - 1) * C + c);
@@ -88,39 +103,30 @@ __global__ void __launch_bounds__(kBlock) column_kernel(const Consts K, const sp
   s.phis0 = __ldg(in.phis0 + c);
   const ZonalRow z = table[c % K.il];
   const uint32_t Sw = __ldg(S);
-  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
-  uint32_t neg = 0;
-  if (verify) {
-#pragma unroll
-    for (int k = 0; k < KX; ++k) {
-      if (q[k] < 0.0f) {
-        neg |= 1u << k;
-        q[k] = 0.0f;
-      }
-    }
-  }
-  ColumnOut<KX> o;
-  column_full<KX>(K, t, q, phi, s, z, Sw, o);
+  ColScalars o;
+  column_smem<KX>(CD, sm, s, z, Sw, o);
+  const float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
+  float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
   // verify_tendencies (physics_interface.py:321-342) with the unclamped humidity
   if (verify) {
     const float dt = K.dt_seconds;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < KX; ++k) {
-      const float qr = (neg >> k & 1u) ? __ldg(in.specific_humidity + (size_t)k * C + c) : q[k];
-      o.dq[k] = (qr + dt * o.dq[k] >= 0.0f) ? o.dq[k] : -qr / dt;
+      const float qr = (neg >> k & 1u) ? __ldg(in.specific_humidity + (size_t)k * C + c)
+                                       : qp[k * kNT];
+      const float dq = dqp[k * kNT];
+      dqp[k * kNT] = (qr + dt * dq >= 0.0f) ? dq : -qr / dt;
     }
   }
-  if (K.q_tend_scale != 1.0f) {
-#pragma unroll
-    for (int k = 0; k < KX; ++k) o.dq[k] = o.dq[k] * K.q_tend_scale;
-  }
-#pragma unroll
+  const float qs = K.q_tend_scale;
+#pragma unroll 4
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
     __stcs(out.u_wind + i, k == KX - 1 ? o.du_low : 0.0f);
     __stcs(out.v_wind + i, k == KX - 1 ? o.dv_low : 0.0f);
-    __stcs(out.temperature + i, o.dt[k]);
-    __stcs(out.specific_humidity + i, o.dq[k]);
+    __stcs(out.temperature + i, dtp[k * kNT]);
+    const float dq = dqp[k * kNT];
+    __stcs(out.specific_humidity + i, qs != 1.0f ? dq * qs : dq);
   }
   __stcs(out.precnv + c, o.precnv);
   __stcs(out.precls + c, o.precls);
@@ -177,21 +183,29 @@ Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_
 }
 
 template <int KX>
-static int launch_fwd(const Consts& K, const spd_inputs_t& in, const spd_outputs_t& out,
+static int launch_fwd(const ConstsD& CD, const spd_inputs_t& in, const spd_outputs_t& out,
                       uint32_t* S, ZonalRow* table, cudaStream_t st) {
-  const int grid = (K.C + kBlock - 1) / kBlock;
+  static bool attr_done = false;  // per template instance; idempotent, so races are harmless
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(column_kernel<KX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<KX>()) != cudaSuccess)
+      return SPD_ERR_CUDA;
+    attr_done = true;
+  }
+  const Consts& K = CD.K;
+  const int grid = (K.C + kNT - 1) / kNT;
   const int grid_a = (max(K.C, K.il) + kBlock - 1) / kBlock;
   cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
-  column_kernel<KX><<<grid, kBlock, 0, st>>>(K, in, out, S, table);
+  column_kernel<KX><<<grid, kNT, smem_bytes<KX>(), st>>>(CD, in, out, S, table);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
-int dispatch_fwd(const Consts& K, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
+int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
                  uint32_t* S, ZonalRow* table, cudaStream_t st) {
   switch (kx) {
-    case 7: return launch_fwd<7>(K, in, out, S, table, st);
-    case 8: return launch_fwd<8>(K, in, out, S, table, st);
-    case 16: return launch_fwd<16>(K, in, out, S, table, st);
+    case 7: return launch_fwd<7>(CD, in, out, S, table, st);
+    case 8: return launch_fwd<8>(CD, in, out, S, table, st);
+    case 16: return launch_fwd<16>(CD, in, out, S, table, st);
     default: return SPD_ERR_KX;
   }
 }
@@ -216,12 +230,14 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
       scratch_bytes < spd_fwd_scratch_bytes(desc))
     return SPD_ERR_SCRATCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const spd::Consts K = spd::make_consts(desc, vgrid, params);
+  spd::ConstsD CD;
+  CD.K = spd::make_consts(desc, vgrid, params);
+  CD.D = spd::derive_constants(desc, vgrid, params);
   uint32_t* S = static_cast<uint32_t*>(scratch);
   spd::ZonalRow* table =
       reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + spd::kHeaderBytes);
   if (cudaMemsetAsync(S, 0, spd::kHeaderBytes, st) != cudaSuccess) return SPD_ERR_CUDA;
-  return spd::dispatch_fwd(K, desc->kx, *in, *out, S, table, st);
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st);
 }
 
 const char* spd_status_string(int status) {

@@ -1,0 +1,624 @@
+// speedy_column_smem.cuh -- the full SPEEDY column, one thread per column, with the per-level
+// arrays of each thread in shared memory ([array][level][thread], stride = block size, so a
+// warp touching one level of one array hits 32 consecutive banks) and the level loops kept
+// rolled.  Compared with a fully unrolled register version this keeps the code small enough
+// for the instruction cache and the register count low; launch-uniform factors come from
+// Derived (host-evaluated).  Expression order follows the reference term by term (file:line
+// relative to the JAX-GCM root); only final scalings by 1/psa use one reciprocal.
+#pragma once
+
+#include "speedy_column.cuh"
+#include "speedy_derived.h"
+
+namespace spd {
+
+constexpr int kNT = 128;  // threads per block = columns per block
+
+// Per-thread level array: element k of this thread lives at p[k * kNT].
+struct Lv {
+  float* p;
+  __device__ __forceinline__ float& operator[](int k) const { return p[k * kNT]; }
+};
+
+enum { A_T, A_Q, A_PHI, A_QSAT, A_RH, A_DT, A_DQ, A_W0, A_W1, A_W2, A_W3, A_W4, kNumArrays };
+
+template <int KX>
+constexpr size_t smem_bytes() {
+  return (size_t)kNumArrays * KX * kNT * sizeof(float);
+}
+
+struct ConstsD {
+  Consts K;
+  Derived D;
+};
+
+struct ColScalars {
+  float du_low, dv_low, precnv, precls, cbmf, cloudc, clstr, rsds, rsns, ftop_sw, rlds, rlns,
+      ftop_lw, tsfc, tskin, shf, evap;
+  int iptop, icltop;
+};
+
+__device__ __forceinline__ float se_at(const Lv& T, const Lv& PHI, int k) {
+  return kCp * T[k] + PHI[k];
+}
+
+// Blackbody emission st4a[k][0..1] (longwave_radiation.py:42-68), from the level temperatures.
+template <int KX>
+__device__ __forceinline__ void st4a_at(const Consts& K, const Lv& T, int k, float& s0,
+                                        float& s1) {
+  const spd_vgrid_t& vg = K.vg;
+  auto th = [&](int j) { return T[j] + vg.wvi[j][1] * (T[j + 1] - T[j]); };
+  if (k == 0) {
+    const float x = 0.75f * T[0] + 0.25f * th(0);
+    s0 = kSbc * (sq(x) * sq(x));
+    s1 = 0.0f;
+  } else if (k == 1) {
+    const float x = 0.50f * T[1] + 0.25f * (th(0) + th(1));
+    s0 = kSbc * (sq(x) * sq(x));
+    s1 = 0.0f;
+  } else {
+    const float t = T[k];
+    const float grad = (k < KX - 1) ? 0.5f * fmaxf(th(k) - th(k - 1), 0.0f)
+                                    : fmaxf(t - th(KX - 2), 0.0f);
+    const float st3 = kSbc * (t * t * t);
+    s0 = st3 * t;
+    s1 = 4.0f * st3 * grad;
+  }
+}
+
+// Longwave band energy fractions (radset, longwave_radiation.py:204-226) times (1 - epslw).
+__device__ __forceinline__ void radset_w(float temp, float w, float fb[4]) {
+  const float j = fminf(fmaxf(temp, 200.0f), 320.0f);
+  const float f1 = 0.148f - 3.0e-6f * sq(j - 247.0f);
+  const float f2 = 0.356f - 5.2e-6f * sq(j - 282.0f);
+  const float f3 = 0.314f + 1.0e-5f * sq(j - 315.0f);
+  const float f0 = 1.0f - (((0.0f + f1) + f2) + f3);
+  fb[0] = w * f0;
+  fb[1] = w * f1;
+  fb[2] = w * f2;
+  fb[3] = w * f3;
+}
+
+template <int KX>
+__device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, const ZonalRow& z,
+                            uint32_t S, ColScalars& o) {
+  const Consts& K = C.K;
+  const Derived& D = C.D;
+  const spd_params_t& p = K.p;
+  const spd_vgrid_t& vg = K.vg;
+  const int tid = threadIdx.x;
+  auto arr = [&](int a) { return Lv{sm + (size_t)a * KX * kNT + tid}; };
+  const Lv T = arr(A_T), Q = arr(A_Q), PHI = arr(A_PHI), QS = arr(A_QSAT), RH = arr(A_RH),
+           DT = arr(A_DT), DQ = arr(A_DQ), W0 = arr(A_W0), W1 = arr(A_W1), W2 = arr(A_W2),
+           W3 = arr(A_W3), W4 = arr(A_W4);
+  const float psa = s.psa;
+  const float rps = 1.0f / psa;
+
+  // ---- spec_hum_to_rel_hum (humidity.py:16-51) --------------------------------------------
+#pragma unroll 4
+  for (int k = 0; k < KX; ++k) {
+    const float qs = qsat_of(T[k], psa, vg.fsg[k]);
+    QS[k] = qs;
+    RH[k] = Q[k] / qs;
+  }
+
+  // ---- set_forcing (physics/speedy/forcing.py:11-39) --------------------------------------
+  const float snowc = fminf(1.0f, s.snowc);
+  const float alb_l = s.alb0 + snowc * (p.albsn - s.alb0);
+  const float alb_s = p.albsea + s.sice * (p.albice - p.albsea);
+  const float albsfc = alb_s + s.fmask * (alb_l - alb_s);
+
+  // ---- diagnose_convection (convection.py:15-97) -------------------------------------------
+  const float q_b = Q[KX - 1], q_b1 = Q[KX - 2];
+  const float se_b = se_at(T, PHI, KX - 1), se_b1 = se_at(T, PHI, KX - 2);
+  int iptop;
+  float qdif = 0.0f;
+  {
+    const float rlhc = (float)(1.0 / 2501.0);
+    const float mse0 = se_b + kAlhc * q_b;
+    const float mse1 = fminf(mse0, se_b1 + kAlhc * q_b1);
+    const float mss0 = fmaxf(mse0, se_b + kAlhc * QS[KX - 1]);
+    int ktop1 = KX, ktop2 = KX;
+    float msthr = 0.0f;
+    float mk1 = se_at(T, PHI, KX - 3) + kAlhc * QS[KX - 3];
+#pragma unroll 1
+    for (int k = KX - 4; k >= 2; --k) {
+      const float mk = se_at(T, PHI, k) + kAlhc * QS[k];
+      const float mss2 = mk + vg.wvi[k][1] * (mk1 - mk);
+      if (mss0 > mss2) ktop1 = k + 1;
+      if (mse1 > mss2) {
+        ktop2 = k + 1;
+        msthr = mss2;
+      }
+      mk1 = mk;
+    }
+    const float qthr0 = p.rhbl * QS[KX - 1];
+    const float qthr1 = p.rhbl * QS[KX - 2];
+    const bool lqthr = (q_b > qthr0) && (q_b1 > qthr1);
+    const bool mask_psa = psa > p.psmin;
+    const bool case1 = mask_psa && (ktop1 < KX) && (ktop2 < KX);
+    const bool case2 = mask_psa && (ktop1 < KX) && !(ktop2 < KX) && lqthr;
+    if (case1) qdif = fmaxf(q_b - qthr0, (mse0 - msthr) * rlhc);
+    if (case2) qdif = q_b - qthr0;
+    iptop = (case1 || case2) ? ktop1 : KX + 1;
+  }
+
+  // ---- get_convection_tendencies (convection.py:99-237) -----------------------------------
+  {
+    const bool mask = iptop < KX;
+    const float qmax = fmaxf(1.01f * q_b, QS[KX - 1]);
+    const float w_last = vg.wvi[KX - 2][1];
+    const float sb = se_b1 + w_last * (se_b - se_b1);
+    const float qb = fminf(q_b1 + w_last * (q_b - q_b1), q_b);
+    const float fpsa = psa * fminf(1.0f, (psa - p.psmin) * D.rdps);
+    const float fmass = D.fm0 * fpsa * fminf(5.0f, qdif / (qmax - qb));
+    const float cbmf = mask ? fmass : 0.0f * fmass;
+    const float fus = fmass * se_b, fuq = fmass * qmax;
+    const float fds = fmass * sb, fdq = fmass * qb;
+    float cm = 0.0f, cs = 0.0f, cq = 0.0f, fsq_sum = 0.0f;
+    float fm_n = 0.f, fus_n = 0.f, fuq_n = 0.f, fds_n = 0.f, fdq_n = 0.f;
+    float dfqa_last = 0.0f, precnv = 0.0f;
+    float se_k = se_b, q_k = q_b;
+#pragma unroll 1
+    for (int k = KX - 1; k >= 0; --k) {
+      const bool lm = (k <= KX - 2) && (k >= iptop);
+      float en = (k >= 1 && k <= KX - 2) ? D.entr[k] * psa * cbmf : 0.0f;
+      en = lm ? en : 0.0f * en;
+      cm = cm + en * 1.0f;
+      cs = cs + en * se_k;
+      cq = cq + en * q_k;
+      const float fm_k = fmass + cm, fus_k = fus + cs, fuq_k = fuq + cq;
+      float se_m = 0.0f, q_m = 0.0f, fds_k, fdq_k;
+      if (k >= 1) {
+        se_m = se_at(T, PHI, k - 1);
+        q_m = Q[k - 1];
+      }
+      if (k == KX - 1) {
+        fds_k = fds;
+        fdq_k = fdq;
+      } else {
+        const float w = (k >= 1) ? vg.wvi[k - 1][1] : 0.0f;
+        const float sb3 = (k >= 1) ? se_m + w * (se_k - se_m) : 0.0f;
+        const float qb3 = (k >= 1) ? q_m + w * (q_k - q_m) : 0.0f;
+        fds_k = fm_k * sb3;
+        fdq_k = fm_k * qb3;
+      }
+      float dfse, dfqa;
+      if (k == KX - 1) {
+        dfse = fds - fus;
+        dfqa = fdq - fuq;
+      } else {
+        const float a = (fus_n - fds_n) - (fus_k - fds_k);
+        const float b = (fuq_n - fdq_n) - (fuq_k - fdq_k);
+        dfse = lm ? a : 0.0f * a;
+        dfqa = lm ? b : 0.0f * b;
+      }
+      const float dq0 = p.rhil * QS[k] - q_k;
+      const float delq = lm ? dq0 : 0.0f * dq0;
+      const float fsq = (delq > 0.0f ? p.smf : 0.0f * p.smf) * cbmf * delq;
+      dfqa = dfqa + fsq;
+      fsq_sum = fsq_sum + fsq;
+      if (k == iptop - 1) {
+        // top layer (detrainment, precipitation), fluxes taken at level iptop = k + 1
+        const float qsatb = QS[k] + vg.wvi[k][1] * (QS[k + 1] - QS[k]);
+        precnv = fmaxf(fuq_n - fm_n * qsatb, 0.0f);
+        dfse = fus_n - fds_n + kAlhc * precnv;
+        dfqa = fuq_n - fdq_n - precnv;
+      }
+      if (k == KX - 1) {
+        dfqa_last = dfqa;
+        DT[k] = dfse * rps * vg.grdscp[k];
+      } else if (k == 0) {
+        DT[0] = dfse;
+        DQ[0] = dfqa;
+      } else {
+        DT[k] = dfse * rps * vg.grdscp[k];
+        DQ[k] = dfqa * rps * vg.grdsig[k];
+      }
+      fm_n = fm_k;
+      fus_n = fus_k;
+      fuq_n = fuq_k;
+      fds_n = fds_k;
+      fdq_n = fdq_k;
+      se_k = se_m;
+      q_k = q_m;
+    }
+    DQ[KX - 1] = (dfqa_last + (-fsq_sum)) * rps * vg.grdsig[KX - 1];
+    o.cbmf = cbmf;
+    o.precnv = precnv;
+  }
+
+  // ---- get_large_scale_condensation_tendencies (large_scale_condensation.py:14-86) --------
+  {
+    const float tfact = (float)(2501.0 / 1004.0);
+    const float psa2 = psa * psa;
+    float psum = 0.0f;
+    int first = 0;
+#pragma unroll 2
+    for (int k = 1; k < KX; ++k) {
+      const float dqa = D.rhref[k] * QS[k] - Q[k];
+      float dql = 0.0f, dtl = 0.0f;
+      if (dqa < 0.0f) {
+        dql = dqa * D.rtlsc;
+        dtl = tfact * fminf(-dql, D.dqmax[k] * psa2);
+        if (first == 0) first = k;
+      }
+      DT[k] = DT[k] + dtl;
+      DQ[k] = DQ[k] + dql;
+      psum = psum + D.pfact[k] * dql;
+    }
+    o.precls = (0.0f - psum) * psa;
+    iptop = min(first == 0 ? 1 : first, iptop);
+  }
+  o.iptop = iptop;
+
+  // ---- clouds (shortwave_radiation.py:313-404) ---------------------------------------------
+  float cloudc, clstr, qcloud;
+  int icltop;
+  {
+    const int nl1 = KX - 2;
+    const float rh_nl1 = RH[nl1];
+    const bool m0 = rh_nl1 > p.rhcl1;
+    const float cloudc0 = m0 ? rh_nl1 - p.rhcl1 : 0.0f;
+    const int icl0 = m0 ? nl1 : KX;
+    float cmax = -INFINITY;
+#pragma unroll 1
+    for (int k = 2; k < KX - 2; ++k) {
+      const float drh = RH[k] - p.rhcl1;
+      const bool m = (drh > cloudc0) && (Q[k] > p.qacl);
+      cmax = fmaxf(cmax, m ? drh : cloudc0);
+    }
+    int icl = -1;
+#pragma unroll 1
+    for (int k = 2; k < KX - 2; ++k) {
+      const float drh = RH[k] - p.rhcl1;
+      const bool m = (drh > cloudc0) && (Q[k] > p.qacl);
+      const float upd = m ? drh : cloudc0;
+      icl = max(icl, (cmax == upd) ? (m ? k : icl0) : icl0);
+    }
+    const float gse = (se_b1 - se_b) / (PHI[KX - 2] - PHI[KX - 1]);
+    const float pr1 = fminf(p.pmaxcl, 86.4f * (o.precnv + o.precls));
+    cloudc = fminf(1.0f, p.wpcl * sqrtf(fmaxf(kEpsilon, pr1)) + sq(fminf(1.0f, cmax * D.rrcl)));
+    if (isnan(cloudc)) cloudc = 1.0f;
+    icltop = min(iptop, icl);
+    qcloud = Q[nl1];
+    const float fstab = fminf(fmaxf(D.rgse * (gse - p.gse_s0), 0.0f), 1.0f);
+    clstr = fstab * fmaxf(p.clsmax - 1.2f * cloudc, 0.0f);
+    const float clstrl = fmaxf(clstr, p.clsminl) * RH[KX - 1];
+    clstr = clstr + s.fmask * (clstrl - clstr);
+  }
+  o.cloudc = cloudc;
+  o.clstr = clstr;
+  o.icltop = icltop;
+
+  // ---- shortwave_rad_fluxes (shortwave_radiation.py:27-217) --------------------------------
+  // W0 = tau band 1, W1 = reflection tau2[:,2], W2 = dfabs
+  float flux_sw0, flux_sw1, rsds;
+  {
+    const bool cmask = icltop < KX;
+    const float refl = cmask ? p.albcl * cloudc : 0.0f;
+    const float psaz = psa * z.zenit;
+    const float acloud = cloudc * fminf(p.abscl1 * qcloud, p.abscl2);
+    W0[0] = expf(-psaz * vg.dhs[0] * p.absdry);
+#pragma unroll 2
+    for (int k = 1; k < KX; ++k) {
+      const float cl = (k >= icltop && k < KX - 1) ? acloud : 0.0f;
+      W0[k] = expf(-psaz * vg.dhs[k] * (D.abs1[k] + p.abswv1 * Q[k] + cl));
+    }
+#pragma unroll 4
+    for (int k = 0; k < KX - 1; ++k) W1[k] = ((S >> k) & 1u) ? refl : 0.0f;
+    W1[KX - 1] = p.albcls * clstr;
+    const float fband2 = 0.05f, fband1 = 0.95f;
+    float f1 = z.fsol * fband1;
+    float d0 = f1;
+    f1 = W0[0] * (f1 - z.ozupp * psa);
+    W2[0] = d0 + (-f1);
+    d0 = f1;
+    f1 = W0[1] * (f1 - z.ozone * psa);
+    W2[1] = d0 + (-f1);
+#pragma unroll 1
+    for (int k = 2; k < KX; ++k) {
+      const float prev = f1, r = W1[k], t0 = W0[k];
+      f1 = prev * t0 * (1.0f - r);
+      W2[k] = prev * (1.0f - r) * (1.0f - t0);
+      W1[k] = r * prev;
+    }
+    float f2 = z.fsol * fband2;
+#pragma unroll 2
+    for (int k = 1; k < KX; ++k) {
+      const float tau1 = expf(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
+      const float prev = f2;
+      f2 = prev * tau1;
+      W2[k] = W2[k] + prev * (1.0f - tau1);
+    }
+    rsds = f1 + f2;
+    float up = f1 * albsfc;
+    o.rsns = rsds - up;
+    const bool gate = (K.model_step % 3) == 0;
+    {
+      const float dlast = W2[KX - 1] + up * (1.0f - W0[KX - 1]);
+      DT[KX - 1] = DT[KX - 1] + (gate ? dlast * vg.grdscp[KX - 1] * rps : 0.0f);
+    }
+#pragma unroll 1
+    for (int k = KX - 1; k >= 1; --k) {
+      up = up * W0[k] + W1[k];
+      const float d = W2[k - 1] + up * (1.0f - W0[k - 1]);
+      DT[k - 1] = DT[k - 1] + (gate ? d * vg.grdscp[k - 1] * rps : 0.0f);
+    }
+    const float ftop_up = W0[0] * up + W1[0];
+    o.ftop_sw = z.fsol - ftop_up;
+    flux_sw0 = ftop_up;
+    flux_sw1 = f2;
+  }
+  o.rsds = rsds;
+
+  // ---- longwave transmissivities (shortwave_radiation.py:174-206): W0..W3 = tau per band ---
+  {
+    const float acl1 = cloudc * p.ablcl1, acl2 = cloudc * p.ablcl2;
+#pragma unroll 2
+    for (int k = 0; k < KX; ++k) {
+      const float qk = Q[k];
+      float a0 = p.ablwin, a2 = p.ablwv1 * qk, a3 = p.ablwv2 * qk;
+      if (k == 0) {
+        a2 = 0.0f;
+        a3 = 0.0f;
+      }
+      if (k >= 2 && k <= KX - 2) {
+        a0 = a0 + ((k > icltop) ? acl1 : acl2);
+        a2 = fmaxf(a2, acl2);
+        a3 = fmaxf(a3, acl2);
+      }
+      W0[k] = expf(-a0 * psa * vg.dhs[k]);
+      W1[k] = expf(-D.ablco2 * psa * vg.dhs[k]);
+      W2[k] = expf(-a2 * psa * vg.dhs[k]);
+      W3[k] = expf(-a3 * psa * vg.dhs[k]);
+    }
+  }
+
+  // ---- get_downward_longwave_rad_fluxes (longwave_radiation.py:13-117): W4 = dfabs --------
+  float rlds;
+  {
+    float fl[4], fb[4], s0, s1;
+    st4a_at<KX>(K, T, 0, s0, s1);
+    radset_w(T[0], D.w_lw, fb);
+    const float tz[4] = {W0[0], W1[0], W2[0], W3[0]};
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const float emis = 1.0f - tz[b];
+      fl[b] = emis * (fb[b] * (s0 + emis * s1));
+    }
+    fl[2] = 0.0f;
+    fl[3] = 0.0f;
+    float sprev = sum4(fl);
+    W4[0] = 0.0f + (-sprev);
+#pragma unroll 1
+    for (int k = 1; k < KX; ++k) {
+      st4a_at<KX>(K, T, k, s0, s1);
+      radset_w(T[k], D.w_lw, fb);
+      const float tk[4] = {W0[k], W1[k], W2[k], W3[k]};
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const float emis = 1.0f - tk[b];
+        fl[b] = tk[b] * fl[b] + emis * (fb[b] * (s0 + emis * s1));
+      }
+      const float sk = sum4(fl);
+      W4[k] = 0.0f + (-(sk - sprev));
+      sprev = sk;
+    }
+    const float ef[4] = {p.emisfc * fl[0], p.emisfc * fl[1], p.emisfc * fl[2], p.emisfc * fl[3]};
+    rlds = sum4(ef);
+    st4a_at<KX>(K, T, KX - 1, s0, s1);
+    const float corlw = D.corlw_f * s0;
+    W4[KX - 1] = W4[KX - 1] + (-corlw);
+    rlds = rlds + corlw;
+  }
+  o.rlds = rlds;
+
+  // ---- get_surface_fluxes (surface_flux.py:15-300) ----------------------------------------
+  float rlus2 = 0.0f, tsfc = 0.0f, tskin_out = 0.0f;
+  {
+    const float ta1 = T[KX - 1], ta2 = T[KX - 2];
+    const float ua = s.u_low, va = s.v_low;
+    const float phi0 = s.orog * kGrav;
+    const float u0 = p.fwind0 * ua, v0 = p.fwind0 * va;
+    float ustr0 = 0.f, ustr1 = 0.f, vstr0 = 0.f, vstr1 = 0.f, shf0 = 0.f;
+    float evap0 = 0.f, rlus0 = 0.f;
+    float t1_1 = 0.f, q1_1 = 0.f, denv2 = 0.f, tskin = 0.f;
+    const bool land = (K.flags & SPD_LFLUXLAND) != 0;
+    if (land) {
+      const float rcp = (float)(1.0 / 1004.0);
+      const float dt1 = vg.wvi[KX - 1][1] * (ta1 - ta2);
+      float t1_0 = 0.0f + (ta1 + dt1);
+      t1_1 = t1_0 - phi0 * dt1 / D.rgas288_sigl;
+      const float t2_1 = ta1 + rcp * PHI[KX - 1];
+      const float t2_0 = t2_1 - rcp * phi0;
+      if (ta1 > ta2) {
+        t1_0 = p.ftemp0 * t1_0 + D.gtemp0 * t2_0;
+        t1_1 = p.ftemp0 * t1_1 + D.gtemp0 * t2_1;
+      } else {
+        t1_0 = ta1;
+        t1_1 = ta1;
+      }
+      const float t0 = t1_1 + s.fmask * (t1_0 - t1_1);
+      const float denv0 =
+          (kP0 * psa / (kRgas * t0)) * sqrtf(u0 * u0 + v0 * v0 + p.vgust * p.vgust);
+      tskin = s.stl + p.ctday * z.sqrt_coa * rsds * (1.0f - alb_l) * psa;
+      const float dthl = (tskin > t2_0) ? fminf(p.dtheta, tskin - t2_0)
+                                        : fmaxf(-p.dtheta, D.astab * (tskin - t2_0));
+      const float denv1 = denv0 * (1.0f + dthl * D.rdth);
+      const float forog = 1.0f + D.rhdrag * (1.0f - expf(-fmaxf(s.phis0, 0.0f) * D.rhdrag));
+      const float cdldv = p.cdl * denv0 * forog;
+      ustr0 = -cdldv * ua;
+      vstr0 = -cdldv * va;
+      shf0 = D.chlcp * denv1 * (tskin - t1_0);
+      const float q1_0 = (p.fhum0 > 0.0f)
+                             ? p.fhum0 * (RH[KX - 1] * qsat_of(t1_0, psa, 1.0f)) + D.ghum0 * q_b
+                             : q_b;
+      const float qs00 = qsat_of(tskin, psa, 1.0f);
+      evap0 = p.chl * denv1 * fmaxf(0.0f, s.soilw * qs00 - q1_0);
+      const float tsk3 = tskin * tskin * tskin;
+      const float drls = 4.0f * D.esbc * tsk3;
+      rlus0 = D.esbc * tsk3 * tskin;
+      float hfl0 = rsds * (1.0f - alb_l) + rlds - (rlus0 + shf0 + (kAlhc * evap0));
+      if (K.flags & SPD_LSKINEB) {
+        const float clamb = p.clambda + (snowc * (p.clambsn - p.clambda));
+        hfl0 = hfl0 - (clamb * (tskin - s.stl));
+        float qs01 = qsat_of(tskin + 1.0f, psa, 1.0f);
+        qs01 = (evap0 > 0.0f) ? s.soilw * (qs01 - qs00) : 0.0f;
+        const float dtskin = hfl0 / (clamb + drls + (p.chl * denv1 * (kCp + (kAlhc * qs01))));
+        tskin = tskin + dtskin;
+        shf0 = shf0 + D.chlcp * denv1 * dtskin;
+        evap0 = evap0 + p.chl * denv1 * qs01 * dtskin;
+        rlus0 = rlus0 + drls * dtskin;
+      }
+      const float sst = s.sst;
+      const float dths = (sst > t2_1) ? fminf(p.dtheta, sst - t2_1)
+                                      : fmaxf(-p.dtheta, D.astab * (sst - t2_1));
+      denv2 = denv0 * (1.0f + dths * D.rdth);
+      q1_1 = (p.fhum0 > 0.0f)
+                 ? p.fhum0 * (RH[KX - 1] * qsat_of(t1_1, psa, 1.0f)) + D.ghum0 * q_b
+                 : q_b;
+      const float cdsdv = p.cds * denv2;
+      ustr1 = -cdsdv * ua;
+      vstr1 = -cdsdv * va;
+    }
+    const float sst = s.sst;
+    const float shf1 = p.chs * kCp * denv2 * (sst - t1_1);
+    const float evap1 = p.chs * denv2 * (qsat_of(sst, psa, 1.0f) - q1_1);
+    const float rlus1 = D.esbc * (sq(sst) * sq(sst));
+    float ustr2 = 0.f, vstr2 = 0.f, shf2 = 0.f, evap2 = 0.f;
+    if (land) {
+      const float fm = s.fmask;
+      ustr2 = ustr1 + fm * (ustr0 - ustr1);
+      vstr2 = vstr1 + fm * (vstr0 - vstr1);
+      shf2 = shf1 + fm * (shf0 - shf1);
+      evap2 = evap1 + fm * (evap0 - evap1);
+      rlus2 = rlus1 + fm * (rlus0 - rlus1);
+      tsfc = sst + fm * (s.stl - sst);
+      tskin_out = sst + fm * (tskin - sst);
+    }
+    o.du_low = 0.0f + ustr2 * rps * vg.grdsig[KX - 1];
+    o.dv_low = 0.0f + vstr2 * rps * vg.grdsig[KX - 1];
+    DT[KX - 1] = DT[KX - 1] + (0.0f + shf2 * rps * vg.grdscp[KX - 1]);
+    DQ[KX - 1] = DQ[KX - 1] + (0.0f + evap2 * rps * vg.grdsig[KX - 1]);
+    o.shf = shf2;
+    o.evap = evap2;
+  }
+  o.tsfc = tsfc;
+  o.tskin = tskin_out;
+
+  // ---- get_upward_longwave_rad_fluxes (longwave_radiation.py:119-202) ---------------------
+  {
+    o.rlns = rlus2 - rlds;
+    float fb[4], fl[4], s0, s1;
+    radset_w(tsfc, D.w_lw, fb);
+    const float fsw[4] = {flux_sw0, flux_sw1, 0.0f, 0.0f};
+#pragma unroll
+    for (int b = 0; b < 4; ++b) fl[b] = fb[b] * rlus2 + D.refsfc * fsw[b];
+    W4[KX - 1] = W4[KX - 1] + p.epslw * rlus2;
+    float sk = sum4(fl);
+#pragma unroll 1
+    for (int k = KX - 1; k >= 1; --k) {
+      st4a_at<KX>(K, T, k, s0, s1);
+      radset_w(T[k], D.w_lw, fb);
+      const float tk[4] = {W0[k], W1[k], W2[k], W3[k]};
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const float emis = 1.0f - tk[b];
+        fl[b] = tk[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1));
+      }
+      const float skm1 = sum4(fl);
+      const float d = W4[k] + (sk - skm1);
+      if (k >= 2) DT[k] = DT[k] + d * vg.grdscp[k] * rps;
+      else W4[k] = d;
+      sk = skm1;
+    }
+    st4a_at<KX>(K, T, 0, s0, s1);
+    float s0b, s1b;
+    st4a_at<KX>(K, T, 1, s0b, s1b);
+    radset_w(T[0], D.w_lw, fb);
+    const float tz[4] = {W0[0], W1[0], W2[0], W3[0]};
+    float top[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const float emis = 1.0f - tz[b];
+      top[b] = (b < 2) ? tz[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1)) : fl[b];
+    }
+    float d0 = W4[0] + ((fl[0] - top[0]) + (fl[1] - top[1]));
+    const float stratc0 = z.stratz * psa, stratc1 = D.eps1 * psa;
+    const float corlw1 = vg.dhs[0] * stratc1 * s0 + stratc0;
+    const float corlw2 = vg.dhs[1] * stratc1 * s0b;
+    d0 = d0 + (-corlw1);
+    const float d1 = W4[1] + (-corlw2);
+    DT[0] = DT[0] + d0 * vg.grdscp[0] * rps;
+    DT[1] = DT[1] + d1 * vg.grdscp[1] * rps;
+    o.ftop_lw = (corlw1 + corlw2) + sum4(top);
+  }
+
+  // ---- get_vertical_diffusion_tend (vertical_diffusion.py:10-136): W0 = tt, W1 = qt --------
+  {
+    const int nl1 = KX - 1;
+    const int icnv = KX - iptop - 1;
+#pragma unroll 4
+    for (int k = 0; k < KX; ++k) {
+      W0[k] = 0.0f;
+      W1[k] = 0.0f;
+    }
+    const float dmse = se_b - se_b1 + kAlhc * (q_b - QS[nl1 - 1]);
+    const float drh = RH[KX - 1] - RH[nl1 - 1];
+    const float fcnv = (icnv > 0 && dmse >= 0.0f) ? p.redshc : 1.0f;
+    if (dmse >= 0.0f) {
+      const float fluxse = fcnv * D.fshcse * dmse;
+      W0[nl1 - 1] = fluxse * D.rsig[nl1 - 1];
+      W0[KX - 1] = -fluxse * D.rsig[KX - 1];
+      if (drh >= 0.0f) {
+        const float fq = fcnv * D.fshcq * QS[KX - 1] * drh;
+        W1[nl1 - 1] = fq * D.rsig[nl1 - 1];
+        W1[KX - 1] = -fq * D.rsig[KX - 1];
+      }
+    } else if (dmse < 0.0f && drh > D.drh0) {
+      const float fq = D.fvdiq2 * QS[nl1 - 1] * drh;
+      W1[nl1 - 1] = fq * D.rsig[nl1 - 1];
+      W1[KX - 1] = -fq * D.rsig[KX - 1];
+    }
+    // moisture diffusion above the PBL: the "+" updates of all levels first, then the "-"
+    float rh_k = RH[2];
+#pragma unroll 1
+    for (int k = 2; k < KX - 2; ++k) {
+      const float rh_n = RH[k + 1];
+      const float dr = rh_n - rh_k;
+      const bool cond = (D.vdcond >> k) & 1u;
+      const float fq = (dr >= D.drh0v[k] && cond) ? D.fvdiq2v[k] * QS[k] * dr : 0.0f;
+      W1[k] = W1[k] + fq * D.rsig[k];
+      W2[k] = fq;
+      rh_k = rh_n;
+    }
+#pragma unroll 1
+    for (int k = 2; k < KX - 2; ++k) W1[k + 1] = W1[k + 1] + (-W2[k] * D.rsig[k + 1]);
+    // damping of super-adiabatic lapse rate: "+" updates first, then the cumulative "-"
+    float se_k = se_at(T, PHI, 0), phi_k = PHI[0];
+#pragma unroll 1
+    for (int k = 0; k < nl1; ++k) {
+      const float se_n = se_at(T, PHI, k + 1), phi_n = PHI[k + 1];
+      const float se0 = se_n - p.segrad * (phi_n - phi_k);
+      const float fse = (se_k < se0) ? D.fvdise * (se0 - se_k) : 0.0f;
+      W0[k] = W0[k] + fse * D.rsig[k];
+      W2[k] = fse;
+      se_k = se_n;
+      phi_k = phi_n;
+    }
+    float cum = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < nl1; ++k) {
+      cum = cum + W2[k] * D.rsig1[k];
+      W0[k + 1] = W0[k + 1] + (-cum);
+    }
+#pragma unroll 4
+    for (int k = 0; k < KX; ++k) {
+      DT[k] = DT[k] + W0[k];
+      DQ[k] = DQ[k] + W1[k];
+    }
+  }
+}
+
+}  // namespace spd

@@ -4,9 +4,24 @@ from __future__ import annotations
 
 import numpy as np
 
-# Parity bar: |cuda - oracle| <= RTOL * max(|oracle|, FLOOR_FRAC * max|oracle field|)
+# Parity bar, per field f:  |cuda - oracle32| <= RTOL * max|oracle32_f|  (normwise, i.e. a
+# per-field absolute floor of RTOL * max|f|).  The float32 oracle itself sits at ~5e-6 of
+# max|f| from the float64 oracle on these fields: the tendencies are sums of terms that cancel,
+# so an elementwise 1e-5 bar would sit below float32's own rounding noise.  In addition the
+# CUDA path's error against the float64 oracle must not exceed X64_FACTOR times the float32
+# oracle's own error against float64, or within X64_FLOOR * max|f|.
+#
+# Diagnostic fields (cloud cover, surface radiation) carry more float32 noise than the
+# tendencies: cloud cover takes sqrt of a precipitation rate that is ~0 in most columns, so the
+# float32 oracle itself sits up to ~5e-5 of max|f| from float64 there.  Their bar is
+# max(RTOL, NOISE_FACTOR * that float32-vs-float64 error), measured on the same inputs.
 RTOL = 1e-5
-FLOOR_FRAC = 1e-3
+NOISE_FACTOR = 2.0
+X64_FACTOR = 3.0
+X64_FLOOR = 1e-5
+STRICT_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity", "precnv", "precls")
+DIAG_FIELDS = ("cloudc", "rsds", "rlds")
+FLOAT_FIELDS = STRICT_FIELDS + DIAG_FIELDS
 
 
 def to_device(pkg, inst, device="cuda"):
@@ -54,8 +69,30 @@ def column_mask(bad, shape2d):
     return b
 
 
-def compare_fields(got, tend, data, rtol=RTOL, floor_frac=FLOOR_FRAC):
+def oracle_f64(inst):
+    """The float64 oracle on the same (float32) input values: state, forcing and geometry
+    fields are widened, vertical tables and parameters are rebuilt in float64."""
+    from oracle import speedy_oracle as O
+    a32 = inst.oracle_args(O.default_parameters())
+    st, fo, ge, da, _ = O.cast_inputs(*a32, np.float64)
+    for n, v in zip(("hsg", "fsg", "dhs", "sigl", "grdsig", "grdscp", "wvi"),
+                    O.vertical_tables(inst.kx, np.float64)):
+        setattr(ge, n, v)
+    return st, fo, ge, da, O.default_parameters(np.float64)
+
+
+def normwise(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
+
+
+def compare_fields(got, tend, data, ref64=None, rtol=RTOL):
+    """Per-field report: normwise error, the tolerance applied and the elementwise failure
+    mask.  ``ref64`` (the float64 oracle's (tend, data)) sets the diagnostic fields' noise-aware
+    tolerance."""
     ref = oracle_fields(tend, data)
+    r64 = oracle_fields(*ref64) if ref64 is not None else None
     rep = {}
     for k, r in ref.items():
         if k not in got:
@@ -64,14 +101,39 @@ def compare_fields(got, tend, data, rtol=RTOL, floor_frac=FLOOR_FRAC):
         r = np.asarray(r, np.float64)
         if k in ("icltop", "iptop"):
             bad = g != r
-            rep[k] = dict(n=r.size, nbad=int(bad.sum()), max_rel=float(bad.mean()), bad=bad)
+            rep[k] = dict(n=r.size, nbad=int(bad.sum()), norm=float(bad.mean()), tol=0.0, bad=bad)
             continue
-        floor = floor_frac * max(np.max(np.abs(r)), 1e-30)
-        denom = np.maximum(np.abs(r), floor)
-        rel = np.abs(g - r) / denom
-        bad = ~(rel <= rtol)
-        rep[k] = dict(n=r.size, nbad=int(bad.sum()), max_rel=float(np.nanmax(rel)), bad=bad)
+        tol = rtol
+        if k in DIAG_FIELDS and r64 is not None:
+            tol = max(rtol, NOISE_FACTOR * normwise(r, r64[k]))
+        scale = max(np.max(np.abs(r)), 1e-30)
+        err = np.abs(g - r)
+        bad = ~(err <= tol * scale)
+        rep[k] = dict(n=r.size, nbad=int(bad.sum()), norm=float(np.nanmax(err) / scale),
+                      tol=tol, bad=bad)
     return rep
+
+
+def x64_errors(got, tend, data, ref64, exclude_cols=None):
+    """Normwise errors of the CUDA path and of the float32 oracle against the float64 oracle,
+    over the columns not in ``exclude_cols`` (trigger flips)."""
+    ref = oracle_fields(tend, data)
+    r64 = oracle_fields(*ref64)
+    out = {}
+    for k in FLOAT_FIELDS:
+        if k not in got:
+            continue
+        g, r, x = (np.asarray(a, np.float64) for a in (got[k], ref[k], r64[k]))
+        if exclude_cols is not None and exclude_cols.any():
+            keep = ~exclude_cols
+            g, r, x = g[..., keep], r[..., keep], x[..., keep]
+        s64 = max(np.max(np.abs(x)), 1e-30)
+        out[k] = (float(np.max(np.abs(g - x)) / s64), float(np.max(np.abs(r - x)) / s64))
+    return out
+
+
+def x64_violations(errs):
+    return {k: v for k, v in errs.items() if v[0] > max(X64_FLOOR, X64_FACTOR * v[1])}
 
 
 def parity_summary(rep, shape2d, margins_ulps=None):
@@ -85,4 +147,5 @@ def parity_summary(rep, shape2d, margins_ulps=None):
         out["flip_columns"] = int(near.sum())
         out["unexplained_columns"] = int((cols & ~(margins_ulps <= 64)).sum())
         out["max_margin_ulps_of_bad"] = float(np.max(margins_ulps[cols])) if cols.any() else 0.0
+    out["_cols"] = cols
     return out

@@ -1,8 +1,12 @@
 """Parity of the CUDA path (through the C ABI) with the NumPy oracle on seeded inputs.
 
-Bar: |cuda - oracle| <= 1e-5 * max(|oracle|, 1e-3 * max|oracle field|) for every tendency
-plane and diagnostic; integer levels (iptop, icltop) exact.  Columns outside the bar must have
-a threshold test within 64 float32 ulps in the oracle (a trigger flip); they are counted.
+Bar, per output field f: |cuda - oracle32| <= tol_f * max|oracle32_f| (a per-field absolute
+floor).  tol_f = 1e-5 for the tendency planes and the precipitation fields; for the diagnostic
+fields (cloud cover, surface radiation) tol_f = max(1e-5, 2x the float32 oracle's own normwise
+error against the float64 oracle on the same inputs).  Integer levels (iptop, icltop) exact.
+Columns outside the bar must have a threshold test within 64 float32 ulps in the oracle (a
+trigger flip); they are counted and bounded.  Over the other columns the CUDA path's normwise
+error against float64 must be within max(1e-5, 3x the float32 oracle's own).
 """
 import importlib
 
@@ -10,7 +14,8 @@ import numpy as np
 import pytest
 
 from oracle import speedy_oracle as O
-from tests.helpers import compare_fields, parity_summary, run_gpu_instance
+from tests.helpers import (compare_fields, oracle_f64, parity_summary, run_gpu_instance,
+                           x64_errors, x64_violations)
 
 pytestmark = pytest.mark.gpu
 
@@ -22,18 +27,20 @@ def pkg():
 
 def check(pkg, inst, params=None, max_flip_frac=2e-3, **kw):
     got = run_gpu_instance(pkg, inst, params=params, **kw)
-    op = O.default_parameters()
-    args = list(inst.oracle_args(op))
+    args = list(inst.oracle_args(O.default_parameters()))
     rec = O.Margins((inst.ix, inst.il))
-    if kw.get("fuse_verify"):
-        tend, data = O.physics_step(*args, rec=rec)
-    else:
-        tend, data = O.compute_tendencies(*args, rec=rec)
-    rep = compare_fields(got, tend, data)
+    step = O.physics_step if kw.get("fuse_verify") else O.compute_tendencies
+    tend, data = step(*args, rec=rec)
+    ref64 = step(*oracle_f64(inst))
+    rep = compare_fields(got, tend, data, ref64)
     summ = parity_summary(rep, (inst.ix, inst.il), rec.ulps)
-    print(inst.name, {k: (v["nbad"], f"{v['max_rel']:.2e}") for k, v in rep.items()}, summ)
+    cols = summ.pop("_cols")
+    x64 = x64_errors(got, tend, data, ref64, exclude_cols=cols)
+    print(inst.name, {k: (v["nbad"], f"{v['norm']:.1e}") for k, v in rep.items()}, summ,
+          {k: (f"{a:.1e}", f"{b:.1e}") for k, (a, b) in x64.items()})
     assert summ["unexplained_columns"] == 0, (summ, {k: v["nbad"] for k, v in rep.items()})
     assert summ["flip_columns"] <= max(2, max_flip_frac * summ["columns"]), summ
+    assert not x64_violations(x64), x64_violations(x64)
     return rep, summ
 
 
