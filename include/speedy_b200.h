@@ -39,7 +39,8 @@ enum spd_status {
   SPD_ERR_SCRATCH = 4,   /* scratch buffer NULL, too small or not 256-byte aligned */
   SPD_ERR_CUDA = 5,      /* a CUDA launch or runtime call failed */
   SPD_ERR_DEVICE = 6,    /* the device reported an error status (bounded wait expired, ...) */
-  SPD_ERR_ALIGN = 7      /* a field pointer is not 16-byte aligned */
+  SPD_ERR_ALIGN = 7,     /* a field pointer is not 16-byte aligned */
+  SPD_ERR_NOALLOC_LIMIT = 8 /* il above SPD_NOALLOC_MAX_IL for spd_fwd_noalloc */
 };
 
 /* spd_desc_t.flags */
@@ -128,6 +129,26 @@ size_t spd_fwd_scratch_bytes(const spd_desc_t* desc);
 int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
             const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
             size_t scratch_bytes, void* stream);
+
+/* ----------------------------------------------------------------------------------------- */
+/* No-allocation variant of spd_fwd.  It has no counterpart in the reference.                 */
+/*                                                                                            */
+/* For callers that cannot allocate device memory or pass a scratch buffer through their      */
+/* binding: a foreign-function bridge that only forwards the state, forcing and tendency      */
+/* buffers it was given, or a process whose device memory belongs to another runtime's        */
+/* pooling allocator.  Same computation and results as spd_fwd, but no scratch argument and   */
+/* no allocation: the scratch lives in a fixed device array of the library (65,792 bytes on   */
+/* every GPU that loads it, kept until process exit), which limits instances to                */
+/* il <= SPD_NOALLOC_MAX_IL latitudes (SPD_ERR_NOALLOC_LIMIT otherwise).                      */
+/*  - The first call on a device looks up the array's device address with that device         */
+/*    current; make that first call before any stream capture.                                */
+/*  - Every call uses the same array and clears its level-set word itself.  Calls whose work   */
+/*    overlaps on the GPU (other streams, other host threads) race on the array and corrupt    */
+/*    each other's results: order them, for example on one stream.                            */
+/* ----------------------------------------------------------------------------------------- */
+#define SPD_NOALLOC_MAX_IL 2048
+int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+                    const spd_inputs_t* in, const spd_outputs_t* out, void* stream);
 
 /* ----------------------------------------------------------------------------------------- */
 /* Helpers                                                                                    */

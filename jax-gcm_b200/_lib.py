@@ -68,7 +68,9 @@ class Outputs(C.Structure):
 
 
 STATUS = {0: "ok", 1: "null pointer", 2: "bad shape", 3: "unsupported kx", 4: "bad scratch",
-          5: "CUDA error", 6: "device error status", 7: "misaligned pointer"}
+          5: "CUDA error", 6: "device error status", 7: "misaligned pointer",
+          8: "il above the no-allocation entry point's limit"}
+NOALLOC_MAX_IL = 2048
 
 _lib = None
 _lock = threading.Lock()
@@ -91,6 +93,9 @@ def _declare(lib):
     lib.spd_abi_version.restype = C.c_int
     lib.spd_default_params.argtypes = [P(Params)]
     lib.spd_default_params.restype = None
+    lib.spd_fwd_noalloc.argtypes = [P(Desc), P(VGrid), P(Params), P(Inputs), P(Outputs),
+                                    C.c_void_p]
+    lib.spd_fwd_noalloc.restype = C.c_int
     for name, spec in EXTRA_DECLS.items():
         fn = getattr(lib, name, None)
         if fn is not None:

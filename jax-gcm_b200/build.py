@@ -7,7 +7,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/speedy_api.cu"]
+SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu"]
 HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
            "../include/speedy_b200.h"]
 OUT = os.path.join(HERE, "libspeedy_b200.so")

@@ -250,6 +250,9 @@ const char* spd_status_string(int status) {
     case SPD_ERR_CUDA: return "CUDA launch or runtime call failed";
     case SPD_ERR_DEVICE: return "device reported an error status";
     case SPD_ERR_ALIGN: return "a field pointer is not 16-byte aligned";
+    case SPD_ERR_NOALLOC_LIMIT:
+      return "instance has more latitudes than spd_fwd_noalloc's fixed scratch holds "
+             "(SPD_NOALLOC_MAX_IL)";
     default: return "unknown status";
   }
 }

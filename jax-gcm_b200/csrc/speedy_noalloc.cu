@@ -1,0 +1,75 @@
+// speedy_noalloc.cu -- spd_fwd_noalloc: the plain forward for callers that cannot allocate.
+//
+// Some callers have no way to obtain device scratch: a foreign-function bridge (cgo, JNI, a
+// ctypes stub) that only forwards the state, forcing and tendency buffers handed to it, or a
+// process whose device memory is owned entirely by another runtime's pooling allocator.  This
+// entry point needs no scratch argument and performs no allocation: its scratch (the
+// instance's cloud-top level set word, a status word and the per-latitude solar table) lives
+// in the fixed file-scope device array below, sized for at most SPD_NOALLOC_MAX_IL latitudes.
+// Every GPU that loads the library keeps that array (65,792 bytes) until the process exits.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "speedy_column_smem.cuh"
+
+namespace spd {
+// Defined in speedy_api.cu.
+int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
+Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
+int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
+                 uint32_t* S, ZonalRow* table, cudaStream_t st);
+}  // namespace spd
+
+namespace {
+
+constexpr size_t kNoallocHeader = 256;  // level-set word, status word, padding
+constexpr size_t kNoallocBytes = kNoallocHeader + (size_t)SPD_NOALLOC_MAX_IL * sizeof(spd::ZonalRow);
+
+// The shared scratch.  In host code this name is only a host-side stand-in for the symbol;
+// its device address comes from cudaGetSymbolAddress (below), once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void* g_dev_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (looked up on first use).
+int scratch_address(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPD_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!g_dev_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SPD_ERR_CUDA;
+    g_dev_ptr[dev] = p;
+  }
+  *out = g_dev_ptr[dev];
+  return SPD_OK;
+}
+
+}  // namespace
+
+extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
+                               const spd_params_t* params, const spd_inputs_t* in,
+                               const spd_outputs_t* out, void* stream) {
+  int rc = spd::check_instance(desc, in, out);
+  if (rc != SPD_OK) return rc;
+  if (!vgrid || !params) return SPD_ERR_NULL;
+  if (desc->il > SPD_NOALLOC_MAX_IL) return SPD_ERR_NOALLOC_LIMIT;
+  void* scratch = nullptr;
+  rc = scratch_address(&scratch);
+  if (rc != SPD_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  spd::ConstsD CD;
+  CD.K = spd::make_consts(desc, vgrid, params);
+  CD.D = spd::derive_constants(desc, vgrid, params);
+  uint32_t* S = static_cast<uint32_t*>(scratch);
+  spd::ZonalRow* table =
+      reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + kNoallocHeader);
+  // The array keeps the previous call's contents: the level-set and status words must start
+  // at zero; the solar table is fully rewritten by the pre-pass.
+  if (cudaMemsetAsync(S, 0, kNoallocHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st);
+}
