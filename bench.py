@@ -40,7 +40,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "t425", "t31"])
-    ap.add_argument("--mode", default="plain", choices=["batched", "plain"])
+    ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -131,7 +132,6 @@ def load_peaks():
 def run_b200(args):
     import torch
     pkg = importlib.import_module("jax-gcm_b200")
-    from tests.helpers import to_device
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -152,7 +152,7 @@ def run_b200(args):
     # device-resident inputs and preallocated outputs
     runs = []
     for m in members:
-        state, forcing, geom, date = to_device(pkg, m, dev)
+        state, forcing, geom, date = pkg.instance_to_device(m, dev)
         phys = pkg.SpeedyPhysics(diagnostics=False)
         e3 = lambda: torch.empty((m.kx, m.ix, m.il), dtype=torch.float32, device=dev)
         e2 = lambda: torch.empty((m.ix, m.il), dtype=torch.float32, device=dev)
@@ -160,11 +160,23 @@ def run_b200(args):
                    precnv=e2(), precls=e2())
         runs.append((m, state, forcing, geom, date, phys, out))
 
-    def step():
+    def step_plain():
         for (_, state, forcing, geom, date, phys, out) in runs:
             phys.compute_tendencies(state, forcing, geom, date, out=out)
 
-    launches_per_step = 2 * len(runs)
+    ens = None
+    if args.mode == "batched":
+        ens = pkg.Ensemble([pkg.Member(st, fo, ge, out) for (_, st, fo, ge, _, _, out) in runs],
+                           runs[0][4])
+        ens.autotune()
+
+        def step():
+            ens.forward()
+
+        launches_per_step = 2
+    else:
+        step = step_plain
+        launches_per_step = 2 * len(runs)
 
     def barrier():
         if dist is not None:
@@ -197,6 +209,12 @@ def run_b200(args):
     clk = clocks.stop()
     ms_step = total_ms / args.steps
     value = cols * world / (ms_step / 1e3)
+    plain = None
+    if args.mode == "batched" and not args.no_plain:
+        pms = timed(step_plain, args.steps, args.warmup) / args.steps
+        plain = {"value": round(cols * world / (pms / 1e3), 1), "ms_per_step": round(pms, 4),
+                 "launches_per_step": 2 * len(runs),
+                 "batched_over_plain": round(pms / ms_step, 2)}
 
     # roofline of the fused forward (cloud-top pre-pass + column kernel), per launch pair
     peak, peak_kind = load_peaks()
@@ -204,7 +222,8 @@ def run_b200(args):
     traffic = NCU_TRAFFIC_PER_COLUMN.get(args.workload)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "kernel": "cloudtop_prepass + column_kernel (one forward)",
+                "kernel": ("ensemble_prepass + ensemble_columns (one step)" if ens is not None
+                           else "cloudtop_prepass + column_kernel (one forward)"),
                 "algorithmic_bytes_per_step": bytes_step,
                 "traffic": (traffic * cols if traffic else None)}
 
@@ -234,7 +253,11 @@ def run_b200(args):
                 state.specific_humidity.copy_(hs["q"], non_blocking=True)
                 state.geopotential.copy_(hs["phi"], non_blocking=True)
                 state.normalized_surface_pressure.copy_(hs["psa"], non_blocking=True)
-                phys.compute_tendencies(state, forcing, geom, date, out=out)
+                if ens is None:
+                    phys.compute_tendencies(state, forcing, geom, date, out=out)
+            if ens is not None:
+                ens.forward()
+            for (hs, ho), (m, state, forcing, geom, date, phys, out) in zip(host, runs):
                 for k, v in ho.items():
                     v.copy_(out[k], non_blocking=True)
             torch.cuda.current_stream().synchronize()
@@ -256,6 +279,7 @@ def run_b200(args):
                 "data": "synthetic (seeded generators with the workload's shapes and distributions)",
                 "config": workload_config(args.workload, members, args.mode),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "plain": plain, "grid_blocks": (ens.grid_blocks if ens is not None else None),
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -131,6 +131,54 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
             size_t scratch_bytes, void* stream);
 
 /* ----------------------------------------------------------------------------------------- */
+/* Batched ragged ensemble: many instances ("members") of mixed resolution and level count,  */
+/* e.g. a forecast ensemble or a set of independent grids, in one pair of persistent launches  */
+/* (cloud-top pre-pass over every member, then the column pass over every member).  Each      */
+/* member gives the same results as spd_fwd on it alone.  There is no reference counterpart   */
+/* for the batching itself; per member it replaces SpeedyPhysics.compute_tendencies           */
+/* (speedy_physics.py:88-127).                                                               */
+/* ----------------------------------------------------------------------------------------- */
+#define SPD_MAX_CLASSES 4
+
+/* What the members of one class share: level count, switches, date (desc; desc.ix/il are
+ * ignored), vertical grid and parameters. */
+typedef struct {
+  spd_desc_t desc;
+  spd_vgrid_t vgrid;
+  spd_params_t params;
+} spd_class_t;
+
+/* One member: its fields (device pointers, spd_fwd layout), shape and class index. */
+typedef struct {
+  spd_inputs_t in;
+  spd_outputs_t out;
+  int32_t ix, il, cls, reserved;
+} spd_member_t;
+
+/* Host-side summary of a plan, returned by spd_ensemble_plan and passed to spd_ensemble_fwd. */
+typedef struct {
+  int32_t nmembers, ntiles;
+  uint64_t levelset_offset, levelset_bytes; /* the per-member level-set words (zeroed per call) */
+  uint64_t plan_bytes;
+} spd_plan_info_t;
+
+/* Bytes of the device plan for these members (member table, tile list, level-set words,
+ * per-member solar tables). */
+size_t spd_ensemble_plan_bytes(const spd_member_t* members, int nmembers);
+
+/* Builds the plan in host memory `plan_host` (plan_bytes long) for a device buffer at
+ * `plan_device` (256-byte aligned); the caller copies plan_host to plan_device once, and may
+ * reuse it for every call while the members' buffers stay where they are. */
+int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member_t* members,
+                      int nmembers, void* plan_host, void* plan_device, size_t plan_bytes,
+                      spd_plan_info_t* info);
+
+/* Runs every member.  grid_blocks = 0 picks SMs x resident blocks; otherwise the persistent
+ * grid size (the autotuner's knob). */
+int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device,
+                     const spd_plan_info_t* info, int grid_blocks, void* stream);
+
+/* ----------------------------------------------------------------------------------------- */
 /* No-allocation variant of spd_fwd.  It has no counterpart in the reference.                 */
 /*                                                                                            */
 /* For callers that cannot allocate device memory or pass a scratch buffer through their      */

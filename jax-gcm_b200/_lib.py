@@ -67,6 +67,23 @@ class Outputs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in OUTPUT_FIELDS]
 
 
+class Class(C.Structure):
+    _fields_ = [("desc", Desc), ("vgrid", VGrid), ("params", Params)]
+
+
+class Member(C.Structure):
+    _fields_ = [("inp", Inputs), ("out", Outputs), ("ix", C.c_int32), ("il", C.c_int32),
+                ("cls", C.c_int32), ("reserved", C.c_int32)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("nmembers", C.c_int32), ("ntiles", C.c_int32),
+                ("levelset_offset", C.c_uint64), ("levelset_bytes", C.c_uint64),
+                ("plan_bytes", C.c_uint64)]
+
+
+MAX_CLASSES = 4
+
 STATUS = {0: "ok", 1: "null pointer", 2: "bad shape", 3: "unsupported kx", 4: "bad scratch",
           5: "CUDA error", 6: "device error status", 7: "misaligned pointer",
           8: "il above the no-allocation entry point's limit"}
@@ -96,6 +113,14 @@ def _declare(lib):
     lib.spd_fwd_noalloc.argtypes = [P(Desc), P(VGrid), P(Params), P(Inputs), P(Outputs),
                                     C.c_void_p]
     lib.spd_fwd_noalloc.restype = C.c_int
+    lib.spd_ensemble_plan_bytes.argtypes = [P(Member), C.c_int]
+    lib.spd_ensemble_plan_bytes.restype = C.c_size_t
+    lib.spd_ensemble_plan.argtypes = [P(Class), C.c_int, P(Member), C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_size_t, P(PlanInfo)]
+    lib.spd_ensemble_plan.restype = C.c_int
+    lib.spd_ensemble_fwd.argtypes = [P(Class), C.c_int, C.c_void_p, P(PlanInfo), C.c_int,
+                                     C.c_void_p]
+    lib.spd_ensemble_fwd.restype = C.c_int
     for name, spec in EXTRA_DECLS.items():
         fn = getattr(lib, name, None)
         if fn is not None:

@@ -1,0 +1,154 @@
+"""Batched ragged ensembles: many grid instances of mixed resolution and level count run in
+one pair of persistent launches (``spd_ensemble_fwd``), optionally captured in a CUDA graph.
+
+Each member gives the same tendencies as ``SpeedyPhysics.compute_tendencies`` on it alone
+(jcm/physics/speedy/speedy_physics.py:88-127); the batching has no reference counterpart.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import List, Optional
+
+import torch
+
+from . import _lib
+from .physics import Parameters, SpeedyPhysics
+
+
+@dataclass
+class Member:
+    state: object      # PhysicsState
+    forcing: object    # ForcingData (2-D or daily 3-D fields)
+    geometry: object   # Geometry
+    out: Optional[dict] = None
+
+
+_TUNE_CACHE = {}
+
+
+class Ensemble:
+    """A fixed set of members whose buffers stay in place between calls.
+
+    ``forward()`` recomputes every member's tendencies into ``member.out`` (dicts with
+    ``u_wind, v_wind, temperature, specific_humidity, precnv, precls``).  Members are grouped
+    into at most four classes by (level count, land-flux switch, vertical grid).
+    """
+
+    def __init__(self, members: List[Member], date, parameters: Optional[Parameters] = None,
+                 fuse_verify=False, time_step=None, q_tend_scale=1.0):
+        lib = _lib.load()
+        self.members = members
+        self.date = date
+        self.phys = SpeedyPhysics(parameters, fuse_verify=fuse_verify, time_step=time_step,
+                                  q_tend_scale=q_tend_scale, diagnostics=False)
+        dev = members[0].state.temperature.device
+        self.device = dev
+        keys, classes = {}, []
+        cls_of = []
+        day = date.model_day()
+        self._keep = []
+        for m in members:
+            g = m.geometry
+            kx = g.nodal_shape[0]
+            key = (kx, bool(m.forcing.lfluxland), tuple(float(x) for x in g.hsg))
+            if key not in keys:
+                if len(classes) == _lib.MAX_CLASSES:
+                    raise ValueError("at most 4 member classes (level count, land flux, grid)")
+                keys[key] = len(classes)
+                c = _lib.Class()
+                c.desc = self.phys.desc(g, date, m.forcing.lfluxland)
+                c.vgrid = g.vgrid()
+                c.params = self.phys._pstruct
+                classes.append(c)
+            cls_of.append(keys[key])
+        self.nclasses = len(classes)
+        self.classes = (_lib.Class * self.nclasses)(*classes)
+        mem = (_lib.Member * len(members))()
+        for i, m in enumerate(members):
+            kx, ix, il = m.geometry.nodal_shape
+            f2 = m.forcing.day_slice(day)
+            self._keep.append(f2)
+            st, g = m.state, m.geometry
+            tensors = dict(u_wind=st.u_wind, v_wind=st.v_wind, temperature=st.temperature,
+                           specific_humidity=st.specific_humidity, geopotential=st.geopotential,
+                           normalized_surface_pressure=st.normalized_surface_pressure,
+                           alb0=f2.alb0, sice_am=f2.sice_am, snowc_am=f2.snowc_am,
+                           soilw_am=f2.soilw_am, stl_am=f2.stl_am,
+                           sea_surface_temperature=f2.sea_surface_temperature, fmask=g.fmask,
+                           orog=g.orog, phis0=g.phis0, sia=g.sia, coa=g.coa)
+            for k, v in tensors.items():
+                if v.dtype != torch.float32 or not v.is_contiguous() or v.device != dev:
+                    raise ValueError(f"member {i}: field {k} must be contiguous float32 on {dev}")
+            if m.out is None:
+                e3 = lambda: torch.empty((kx, ix, il), dtype=torch.float32, device=dev)
+                e2 = lambda: torch.empty((ix, il), dtype=torch.float32, device=dev)
+                m.out = dict(u_wind=e3(), v_wind=e3(), temperature=e3(), specific_humidity=e3(),
+                             precnv=e2(), precls=e2())
+            mem[i].inp = _lib.Inputs(**{k: tensors[k].data_ptr() for k in _lib.INPUT_FIELDS})
+            mem[i].out = _lib.Outputs(**{k: (m.out[k].data_ptr() if k in m.out else None)
+                                         for k in _lib.OUTPUT_FIELDS})
+            mem[i].ix, mem[i].il, mem[i].cls = ix, il, cls_of[i]
+        self._members_c = mem
+        nbytes = lib.spd_ensemble_plan_bytes(mem, len(members))
+        self.plan = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        host = (C.c_ubyte * nbytes)()
+        self.info = _lib.PlanInfo()
+        rc = lib.spd_ensemble_plan(self.classes, self.nclasses, mem, len(members),
+                                   C.cast(host, C.c_void_p), C.c_void_p(self.plan.data_ptr()),
+                                   nbytes, C.byref(self.info))
+        _lib.check(rc, "spd_ensemble_plan")
+        self.plan.copy_(torch.frombuffer(bytearray(host), dtype=torch.uint8))
+        self.grid_blocks = 0
+        self.columns = sum(m.geometry.nodal_shape[1] * m.geometry.nodal_shape[2] for m in members)
+
+    def signature(self):
+        return tuple(sorted((m.geometry.nodal_shape for m in self.members)))
+
+    def forward(self, grid_blocks=None):
+        lib = _lib.load()
+        gb = self.grid_blocks if grid_blocks is None else grid_blocks
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        rc = lib.spd_ensemble_fwd(self.classes, self.nclasses, C.c_void_p(self.plan.data_ptr()),
+                                  C.byref(self.info), int(gb), C.c_void_p(stream))
+        _lib.check(rc, "spd_ensemble_fwd")
+        return [m.out for m in self.members]
+
+    def autotune(self, candidates=None, reps=5):
+        """Picks the persistent grid size by timing the candidates (CUDA events); cached per
+        ensemble signature."""
+        sig = self.signature()
+        if sig in _TUNE_CACHE:
+            self.grid_blocks = _TUNE_CACHE[sig]
+            return self.grid_blocks
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        cands = candidates or [0, sms, 2 * sms, 3 * sms, 4 * sms]
+        best, best_ms = 0, float("inf")
+        for gb in cands:
+            self.forward(gb)
+            torch.cuda.synchronize(self.device)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.forward(gb)
+            b.record()
+            torch.cuda.synchronize(self.device)
+            ms = a.elapsed_time(b) / reps
+            if ms < best_ms:
+                best, best_ms = gb, ms
+        self.grid_blocks = best
+        _TUNE_CACHE[sig] = best
+        return best
+
+    def capture(self, calls=1):
+        """A CUDA graph of ``calls`` consecutive forwards (replay with ``graph.replay()``)."""
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.forward()
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for _ in range(calls):
+                self.forward()
+        return g

@@ -7,8 +7,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu"]
+SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu", "csrc/speedy_ensemble.cu"]
 HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
+           "csrc/speedy_kernels.cuh",
            "../include/speedy_b200.h"]
 OUT = os.path.join(HERE, "libspeedy_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -5,38 +5,15 @@
 //      instance ORs them into one 32-bit level set S (the cross-column dependency of
 //      shortwave_radiation.py:62-68); the same launch writes the per-latitude solar table.
 //   2. column_kernel: the fused physics of every column (speedy_physics.py:88-127), reading S.
-// One thread owns one column; the per-level fields live in registers.
+// One thread owns one column (speedy_kernels.cuh, speedy_column_smem.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "speedy_column_smem.cuh"
+#include "speedy_kernels.cuh"
 
 namespace spd {
 
-constexpr int kBlock = 128;
 constexpr size_t kHeaderBytes = 256;  // S word, status word, padding
-
-template <int KX>
-__device__ __forceinline__ void load_levels(const float* __restrict__ f, int C, int c, float v[KX]) {
-#pragma unroll
-  for (int k = 0; k < KX; ++k) v[k] = __ldg(f + (size_t)k * C + c);
-}
-
-// Level set of one block, OR-ed into the instance word once per block.
-__device__ __forceinline__ void or_level_set(uint32_t bit, uint32_t* S) {
-  __shared__ uint32_t warp_bits[kBlock / 32];
-  bit = __reduce_or_sync(0xffffffffu, bit);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) warp_bits[warp] = bit;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t b = 0;
-#pragma unroll
-    for (int w = 0; w < kBlock / 32; ++w) b |= warp_bits[w];
-    const uint32_t have = *reinterpret_cast<volatile uint32_t*>(S);
-    if ((have & b) != b) atomicOr(S, b);
-  }
-}
 
 template <int KX>
 __global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const spd_inputs_t in,
@@ -44,20 +21,7 @@ __global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const
                                                            ZonalRow* __restrict__ table) {
   const int c = blockIdx.x * kBlock + threadIdx.x;
   if (c < K.il) table[c] = zonal_row(K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
-  uint32_t bit = 0;
-  if (c < K.C) {
-    float t[KX], q[KX], phi[KX];
-    load_levels<KX>(in.temperature, K.C, c, t);
-    load_levels<KX>(in.specific_humidity, K.C, c, q);
-    load_levels<KX>(in.geopotential, K.C, c, phi);
-    if (K.flags & SPD_FUSE_VERIFY) {
-#pragma unroll
-      for (int k = 0; k < KX; ++k) q[k] = (q[k] < 0.0f) ? 0.0f : q[k];
-    }
-    const float psa = __ldg(in.normalized_surface_pressure + c);
-    const int icl = column_icltop<KX>(K, t, q, phi, psa);
-    bit = 1u << min(max(icl, 0), KX - 1);
-  }
+  const uint32_t bit = (c < K.C) ? prepass_column<KX>(K, in, c, K.C) : 0u;
   or_level_set(bit, S);
 }
 
@@ -67,84 +31,9 @@ __global__ void __launch_bounds__(kNT, 2) column_kernel(const ConstsD CD, const 
                                                         const uint32_t* __restrict__ S,
                                                         const ZonalRow* __restrict__ table) {
   extern __shared__ float sm[];
-  const Consts& K = CD.K;
   const int c = blockIdx.x * kNT + threadIdx.x;
-  if (c >= K.C) return;
-  const int C = K.C;
-  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
-  float* tp = sm + (size_t)A_T * KX * kNT + threadIdx.x;
-  float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
-  float* pp = sm + (size_t)A_PHI * KX * kNT + threadIdx.x;
-  uint32_t neg = 0;
-#pragma unroll 4
-  for (int k = 0; k < KX; ++k) {
-    const size_t i = (size_t)k * C + c;
-    tp[k * kNT] = __ldg(in.temperature + i);
-    float q = __ldg(in.specific_humidity + i);
-    if (verify && q < 0.0f) {
-      neg |= 1u << k;
-      q = 0.0f;
-    }
-    qp[k * kNT] = q;
-    pp[k * kNT] = __ldg(in.geopotential + i);
-  }
-  SurfaceIn s;
-  s.psa = __ldg(in.normalized_surface_pressure + c);
-  s.u_low = __ldg(in.u_wind + (size_t)(KX - 1) * C + c);
-  s.v_low = __ldg(in.v_wind + (size_t)(KX - 1) * C + c);
-  s.sst = __ldg(in.sea_surface_temperature + c);
-  s.stl = __ldg(in.stl_am + c);
-  s.soilw = __ldg(in.soilw_am + c);
-  s.snowc = __ldg(in.snowc_am + c);
-  s.sice = __ldg(in.sice_am + c);
-  s.alb0 = __ldg(in.alb0 + c);
-  s.fmask = __ldg(in.fmask + c);
-  s.orog = __ldg(in.orog + c);
-  s.phis0 = __ldg(in.phis0 + c);
-  const ZonalRow z = table[c % K.il];
-  const uint32_t Sw = __ldg(S);
-  ColScalars o;
-  column_smem<KX>(CD, sm, s, z, Sw, o);
-  const float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
-  float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
-  // verify_tendencies (physics_interface.py:321-342) with the unclamped humidity
-  if (verify) {
-    const float dt = K.dt_seconds;
-#pragma unroll 1
-    for (int k = 0; k < KX; ++k) {
-      const float qr = (neg >> k & 1u) ? __ldg(in.specific_humidity + (size_t)k * C + c)
-                                       : qp[k * kNT];
-      const float dq = dqp[k * kNT];
-      dqp[k * kNT] = (qr + dt * dq >= 0.0f) ? dq : -qr / dt;
-    }
-  }
-  const float qs = K.q_tend_scale;
-#pragma unroll 4
-  for (int k = 0; k < KX; ++k) {
-    const size_t i = (size_t)k * C + c;
-    __stcs(out.u_wind + i, k == KX - 1 ? o.du_low : 0.0f);
-    __stcs(out.v_wind + i, k == KX - 1 ? o.dv_low : 0.0f);
-    __stcs(out.temperature + i, dtp[k * kNT]);
-    const float dq = dqp[k * kNT];
-    __stcs(out.specific_humidity + i, qs != 1.0f ? dq * qs : dq);
-  }
-  __stcs(out.precnv + c, o.precnv);
-  __stcs(out.precls + c, o.precls);
-  if (out.cbmf) out.cbmf[c] = o.cbmf;
-  if (out.cloudc) out.cloudc[c] = o.cloudc;
-  if (out.cloudstr) out.cloudstr[c] = o.clstr;
-  if (out.rsds) out.rsds[c] = o.rsds;
-  if (out.rsns) out.rsns[c] = o.rsns;
-  if (out.ftop_sw) out.ftop_sw[c] = o.ftop_sw;
-  if (out.rlds) out.rlds[c] = o.rlds;
-  if (out.rlns) out.rlns[c] = o.rlns;
-  if (out.ftop_lw) out.ftop_lw[c] = o.ftop_lw;
-  if (out.tsfc) out.tsfc[c] = o.tsfc;
-  if (out.tskin) out.tskin[c] = o.tskin;
-  if (out.shf) out.shf[c] = o.shf;
-  if (out.evap) out.evap[c] = o.evap;
-  if (out.iptop) out.iptop[c] = o.iptop;
-  if (out.icltop) out.icltop[c] = o.icltop;
+  if (c >= CD.K.C) return;
+  column_process<KX>(CD, sm, in, out, __ldg(S), table, c, CD.K.C, CD.K.il);
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }

@@ -1,0 +1,214 @@
+// speedy_ensemble.cu -- the batched ragged ensemble: many members of mixed resolution and
+// level count in two persistent launches over one tile list.
+//
+// A member is one grid instance (its own arrays, ix*il columns, kx levels).  The plan splits
+// every member into tiles of kNT consecutive columns (a tile never straddles members), ordered
+// by level count (16-level tiles first, the heavier work), and keeps per member the field
+// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 is the
+// cloud-top pre-pass over all tiles (each member's level set and solar table, as in
+// spd_fwd's first launch); launch 2 runs the full column body on all tiles, reading each
+// member's level set.  Both launches are persistent: gridDim blocks stride over the tile list.
+// Constants shared by a class of members (kx, date, switches, vertical grid, parameters) travel
+// by value in the kernel parameters.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "speedy_kernels.cuh"
+
+namespace spd {
+
+int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
+Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
+
+struct MemberDev {
+  spd_inputs_t in;
+  spd_outputs_t out;
+  int C, il, kx, cls;
+  uint32_t* S;
+  ZonalRow* table;
+};
+
+struct ClassArgs {
+  ConstsD cls[SPD_MAX_CLASSES];
+};
+
+struct Tile {
+  int member, col0;
+};
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <int KX>
+__device__ __forceinline__ void prepass_tile(const ClassArgs& A, const MemberDev& m, int c) {
+  const Consts& K = A.cls[m.cls].K;
+  if (c < m.il) m.table[c] = zonal_row(K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
+  const uint32_t bit = (c < m.C) ? prepass_column<KX>(K, m.in, c, m.C) : 0u;
+  or_level_set(bit, m.S);
+}
+
+__global__ void __launch_bounds__(kBlock) ensemble_prepass(const __grid_constant__ ClassArgs A,
+                                                           const MemberDev* __restrict__ members,
+                                                           const Tile* __restrict__ tiles,
+                                                           int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const MemberDev& m = members[tl.member];
+    const int c = tl.col0 + threadIdx.x;
+    switch (m.kx) {  // uniform per block
+      case 16: prepass_tile<16>(A, m, c); break;
+      case 8: prepass_tile<8>(A, m, c); break;
+      default: prepass_tile<7>(A, m, c); break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kNT, 2) ensemble_columns(const __grid_constant__ ClassArgs A,
+                                                           const MemberDev* __restrict__ members,
+                                                           const Tile* __restrict__ tiles,
+                                                           int ntiles) {
+  extern __shared__ float sm[];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const MemberDev& m = members[tl.member];
+    const int c = tl.col0 + threadIdx.x;
+    if (c < m.C) {
+      const ConstsD& CD = A.cls[m.cls];
+      const uint32_t Sw = *m.S;
+      switch (m.kx) {
+        case 16: column_process<16>(CD, sm, m.in, m.out, Sw, m.table, c, m.C, m.il); break;
+        case 8: column_process<8>(CD, sm, m.in, m.out, Sw, m.table, c, m.C, m.il); break;
+        default: column_process<7>(CD, sm, m.in, m.out, Sw, m.table, c, m.C, m.il); break;
+      }
+    }
+  }
+}
+
+struct Layout {
+  size_t members, tiles, levelset, tables, total;
+  int ntiles;
+};
+
+static Layout layout_of(const spd_member_t* members, int n) {
+  Layout L;
+  int ntiles = 0;
+  size_t tab = 0;
+  for (int i = 0; i < n; ++i) {
+    const int C = members[i].ix * members[i].il;
+    ntiles += (C + kNT - 1) / kNT;
+    tab += align256((size_t)members[i].il * sizeof(ZonalRow));
+  }
+  L.ntiles = ntiles;
+  L.members = 256;
+  L.tiles = L.members + align256((size_t)n * sizeof(MemberDev));
+  L.levelset = L.tiles + align256((size_t)ntiles * sizeof(Tile));
+  L.tables = L.levelset + align256((size_t)n * sizeof(uint32_t));
+  L.total = L.tables + tab;
+  return L;
+}
+
+}  // namespace spd
+
+extern "C" {
+
+size_t spd_ensemble_plan_bytes(const spd_member_t* members, int nmembers) {
+  if (!members || nmembers <= 0) return 0;
+  return spd::layout_of(members, nmembers).total;
+}
+
+int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member_t* members,
+                      int nmembers, void* plan_host, void* plan_device, size_t plan_bytes,
+                      spd_plan_info_t* info) {
+  using namespace spd;
+  if (!classes || !members || !plan_host || !plan_device || !info) return SPD_ERR_NULL;
+  if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || nmembers <= 0) return SPD_ERR_SHAPE;
+  if (reinterpret_cast<uintptr_t>(plan_device) & 255u) return SPD_ERR_SCRATCH;
+  const Layout L = layout_of(members, nmembers);
+  if (plan_bytes < L.total) return SPD_ERR_SCRATCH;
+  for (int i = 0; i < nmembers; ++i) {
+    const spd_member_t& m = members[i];
+    if (m.cls < 0 || m.cls >= nclasses) return SPD_ERR_SHAPE;
+    spd_desc_t d = classes[m.cls].desc;
+    d.ix = m.ix;
+    d.il = m.il;
+    const int rc = check_instance(&d, &m.in, &m.out);
+    if (rc != SPD_OK) return rc;
+  }
+  char* h = static_cast<char*>(plan_host);
+  char* dbase = static_cast<char*>(plan_device);
+  memset(h, 0, L.total);
+  MemberDev* md = reinterpret_cast<MemberDev*>(h + L.members);
+  size_t tab = L.tables;
+  for (int i = 0; i < nmembers; ++i) {
+    const spd_member_t& m = members[i];
+    md[i].in = m.in;
+    md[i].out = m.out;
+    md[i].C = m.ix * m.il;
+    md[i].il = m.il;
+    md[i].kx = classes[m.cls].desc.kx;
+    md[i].cls = m.cls;
+    md[i].S = reinterpret_cast<uint32_t*>(dbase + L.levelset) + i;
+    md[i].table = reinterpret_cast<ZonalRow*>(dbase + tab);
+    tab += align256((size_t)m.il * sizeof(ZonalRow));
+  }
+  // tiles: 16-level members first, then fewer levels (heavier work first)
+  std::vector<int> order(nmembers);
+  for (int i = 0; i < nmembers; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return md[a].kx > md[b].kx; });
+  Tile* tl = reinterpret_cast<Tile*>(h + L.tiles);
+  int t = 0;
+  for (int i : order)
+    for (int c0 = 0; c0 < md[i].C; c0 += kNT) tl[t++] = Tile{i, c0};
+  info->nmembers = nmembers;
+  info->ntiles = t;
+  info->levelset_offset = L.levelset;
+  info->levelset_bytes = align256((size_t)nmembers * sizeof(uint32_t));
+  info->plan_bytes = L.total;
+  return SPD_OK;
+}
+
+int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device,
+                     const spd_plan_info_t* info, int grid_blocks, void* stream) {
+  using namespace spd;
+  if (!classes || !plan_device || !info) return SPD_ERR_NULL;
+  if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
+  static bool attr_done = false;
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<16>()) != cudaSuccess)
+      return SPD_ERR_CUDA;
+    attr_done = true;
+  }
+  ClassArgs A;
+  for (int i = 0; i < nclasses; ++i) {
+    A.cls[i].K = make_consts(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+    A.cls[i].D = derive_constants(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+  }
+  int grid = grid_blocks;
+  if (grid <= 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_columns, kNT,
+                                                      smem_bytes<16>()) != cudaSuccess)
+      return SPD_ERR_CUDA;
+    grid = sms * std::max(per_sm, 1);
+  }
+  grid = std::min(grid, info->ntiles);
+  char* base = static_cast<char*>(plan_device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const MemberDev* md = reinterpret_cast<const MemberDev*>(base + 256);
+  const size_t tiles_off = 256 + align256((size_t)info->nmembers * sizeof(MemberDev));
+  const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
+  if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
+    return SPD_ERR_CUDA;
+  ensemble_prepass<<<grid * 2, kBlock, 0, st>>>(A, md, tl, info->ntiles);
+  ensemble_columns<<<grid, kNT, smem_bytes<16>(), st>>>(A, md, tl, info->ntiles);
+  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -521,3 +521,19 @@ def get_physical_tendencies_columns(state, physics, forcing, geometry, date, tim
         q_tend_scale=physics.q_tend_scale, diagnostics=physics.diagnostics)
     phys.time_step = time_step
     return phys.compute_tendencies(state, forcing, geometry, date)
+
+
+def instance_to_device(inst, device="cuda"):
+    """(PhysicsState, ForcingData, Geometry, DateData) on ``device`` for a synthetic Instance
+    (``synthetic.py``)."""
+    dev = torch.device(device)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
+    state = PhysicsState(t(inst.u), t(inst.v), t(inst.t), t(inst.q), t(inst.phi), t(inst.psa))
+    forcing = ForcingData(t(inst.alb0), t(inst.sice), t(inst.snowc), t(inst.soilw),
+                          t(inst.stl), t(inst.sst), lfluxland=inst.lfluxland)
+    geom = Geometry.from_grid_shape((inst.ix, inst.il), inst.kx, orography=inst.orog,
+                                    fmask=inst.fmask, phis0=inst.phis0, latitudes=inst.lat,
+                                    device=dev)
+    geom.sia, geom.coa = t(inst.sia), t(inst.coa)
+    date = DateData(inst.tyear, inst.model_year, inst.model_step, inst.dt_seconds)
+    return state, forcing, geom, date

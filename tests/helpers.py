@@ -25,18 +25,7 @@ FLOAT_FIELDS = STRICT_FIELDS + DIAG_FIELDS
 
 
 def to_device(pkg, inst, device="cuda"):
-    import torch
-    dev = torch.device(device)
-    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float32, device=dev)
-    state = pkg.PhysicsState(t(inst.u), t(inst.v), t(inst.t), t(inst.q), t(inst.phi), t(inst.psa))
-    forcing = pkg.ForcingData(t(inst.alb0), t(inst.sice), t(inst.snowc), t(inst.soilw),
-                              t(inst.stl), t(inst.sst), lfluxland=inst.lfluxland)
-    geom = pkg.Geometry.from_grid_shape((inst.ix, inst.il), inst.kx, orography=inst.orog,
-                                        fmask=inst.fmask, phis0=inst.phis0, latitudes=inst.lat,
-                                        device=dev)
-    geom.sia, geom.coa = t(inst.sia), t(inst.coa)
-    date = pkg.DateData(inst.tyear, inst.model_year, inst.model_step, inst.dt_seconds)
-    return state, forcing, geom, date
+    return pkg.instance_to_device(inst, device)
 
 
 def run_gpu_instance(pkg, inst, device="cuda", params=None, **kw):
