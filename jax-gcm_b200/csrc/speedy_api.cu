@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const
 }
 
 template <int KX>
-__global__ void __launch_bounds__(kNT, 2) column_kernel(const ConstsD CD, const spd_inputs_t in,
+__global__ void __launch_bounds__(kNT, 4) column_kernel(const ConstsD CD, const spd_inputs_t in,
                                                         const spd_outputs_t out,
                                                         const uint32_t* __restrict__ S,
                                                         const ZonalRow* __restrict__ table) {

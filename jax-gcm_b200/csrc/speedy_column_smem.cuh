@@ -3,8 +3,19 @@
 // warp touching one level of one array hits 32 consecutive banks) and the level loops kept
 // rolled.  Compared with a fully unrolled register version this keeps the code small enough
 // for the instruction cache and the register count low; launch-uniform factors come from
-// Derived (host-evaluated).  Expression order follows the reference term by term (file:line
-// relative to the JAX-GCM root); only final scalings by 1/psa use one reciprocal.
+// Derived (host-evaluated).
+//
+// Shared memory per thread is the occupancy limit, so only seven level arrays are kept (T, q,
+// phi, qsat, the two tendency accumulators and one work array, 56 KB per 128-column block at
+// 16 levels -> four blocks per SM): relative humidity is recomputed as q/qsat where used, the
+// longwave transmissivities are recomputed in the upward pass, the shortwave and longwave
+// absorbed fluxes are added to the temperature accumulator as each piece completes, and the
+// vertical-diffusion terms are formed level by level in one ascending pass.
+//
+// Expression order follows the reference term by term (file:line relative to the JAX-GCM
+// root).  Deviations, all at the rounding level and never inside a cancelling difference:
+// final scalings by 1/psa use one reciprocal, and the radiative absorbed-flux pieces of a
+// level are scaled and added one at a time instead of summed first.
 #pragma once
 
 #include "speedy_column.cuh"
@@ -20,7 +31,7 @@ struct Lv {
   __device__ __forceinline__ float& operator[](int k) const { return p[k * kNT]; }
 };
 
-enum { A_T, A_Q, A_PHI, A_QSAT, A_RH, A_DT, A_DQ, A_W0, A_W1, A_W2, A_W3, A_W4, kNumArrays };
+enum { A_T, A_Q, A_PHI, A_QSAT, A_DT, A_DQ, A_W, kNumArrays };
 
 template <int KX>
 constexpr size_t smem_bytes() {
@@ -88,19 +99,15 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
   const spd_vgrid_t& vg = K.vg;
   const int tid = threadIdx.x;
   auto arr = [&](int a) { return Lv{sm + (size_t)a * KX * kNT + tid}; };
-  const Lv T = arr(A_T), Q = arr(A_Q), PHI = arr(A_PHI), QS = arr(A_QSAT), RH = arr(A_RH),
-           DT = arr(A_DT), DQ = arr(A_DQ), W0 = arr(A_W0), W1 = arr(A_W1), W2 = arr(A_W2),
-           W3 = arr(A_W3), W4 = arr(A_W4);
+  const Lv T = arr(A_T), Q = arr(A_Q), PHI = arr(A_PHI), QS = arr(A_QSAT), DT = arr(A_DT),
+           DQ = arr(A_DQ), W = arr(A_W);
+  auto rh_at = [&](int k) { return Q[k] / QS[k]; };  // spec_hum_to_rel_hum (humidity.py:45)
   const float psa = s.psa;
   const float rps = 1.0f / psa;
 
   // ---- spec_hum_to_rel_hum (humidity.py:16-51) --------------------------------------------
 #pragma unroll 4
-  for (int k = 0; k < KX; ++k) {
-    const float qs = qsat_of(T[k], psa, vg.fsg[k]);
-    QS[k] = qs;
-    RH[k] = Q[k] / qs;
-  }
+  for (int k = 0; k < KX; ++k) QS[k] = qsat_of(T[k], psa, vg.fsg[k]);
 
   // ---- set_forcing (physics/speedy/forcing.py:11-39) --------------------------------------
   const float snowc = fminf(1.0f, s.snowc);
@@ -257,25 +264,25 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
   int icltop;
   {
     const int nl1 = KX - 2;
-    const float rh_nl1 = RH[nl1];
+    const float rh_nl1 = rh_at(nl1);
     const bool m0 = rh_nl1 > p.rhcl1;
     const float cloudc0 = m0 ? rh_nl1 - p.rhcl1 : 0.0f;
     const int icl0 = m0 ? nl1 : KX;
-    float cmax = -INFINITY;
+    // Lines 365-373 take, over k = 2..kx-3, the max of (cmax == upd_k ? (m_k ? k : icl0) : icl0)
+    // with icl0 >= kx-2 > k.  That max is kx-3 exactly when every level has m_k and
+    // upd_k == cmax (i.e. all m_k and min upd == max upd), and icl0 otherwise: one pass.
+    float cmax = -INFINITY, cmin = INFINITY;
+    bool allm = true;
 #pragma unroll 1
     for (int k = 2; k < KX - 2; ++k) {
-      const float drh = RH[k] - p.rhcl1;
-      const bool m = (drh > cloudc0) && (Q[k] > p.qacl);
-      cmax = fmaxf(cmax, m ? drh : cloudc0);
-    }
-    int icl = -1;
-#pragma unroll 1
-    for (int k = 2; k < KX - 2; ++k) {
-      const float drh = RH[k] - p.rhcl1;
+      const float drh = rh_at(k) - p.rhcl1;
       const bool m = (drh > cloudc0) && (Q[k] > p.qacl);
       const float upd = m ? drh : cloudc0;
-      icl = max(icl, (cmax == upd) ? (m ? k : icl0) : icl0);
+      cmax = fmaxf(cmax, upd);
+      cmin = fminf(cmin, upd);
+      allm = allm && m;
     }
+    const int icl = (allm && cmin == cmax) ? KX - 3 : icl0;
     const float gse = (se_b1 - se_b) / (PHI[KX - 2] - PHI[KX - 1]);
     const float pr1 = fminf(p.pmaxcl, 86.4f * (o.precnv + o.precls));
     cloudc = fminf(1.0f, p.wpcl * sqrtf(fmaxf(kEpsilon, pr1)) + sq(fminf(1.0f, cmax * D.rrcl)));
@@ -284,133 +291,133 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
     qcloud = Q[nl1];
     const float fstab = fminf(fmaxf(D.rgse * (gse - p.gse_s0), 0.0f), 1.0f);
     clstr = fstab * fmaxf(p.clsmax - 1.2f * cloudc, 0.0f);
-    const float clstrl = fmaxf(clstr, p.clsminl) * RH[KX - 1];
+    const float clstrl = fmaxf(clstr, p.clsminl) * rh_at(KX - 1);
     clstr = clstr + s.fmask * (clstrl - clstr);
   }
   o.cloudc = cloudc;
   o.clstr = clstr;
   o.icltop = icltop;
 
-  // ---- shortwave_rad_fluxes (shortwave_radiation.py:27-217) --------------------------------
-  // W0 = tau band 1, W1 = reflection tau2[:,2], W2 = dfabs
+  // ---- shortwave_rad_fluxes (shortwave_radiation.py:27-217); W = reflection tau2[:,2] -------
   float flux_sw0, flux_sw1, rsds;
   {
     const bool cmask = icltop < KX;
     const float refl = cmask ? p.albcl * cloudc : 0.0f;
     const float psaz = psa * z.zenit;
     const float acloud = cloudc * fminf(p.abscl1 * qcloud, p.abscl2);
-    W0[0] = expf(-psaz * vg.dhs[0] * p.absdry);
-#pragma unroll 2
-    for (int k = 1; k < KX; ++k) {
+    const bool gate = (K.model_step % 3) == 0;
+    // band-1 transmissivity of level k (lines 80-94)
+    auto tau0_at = [&](int k) {
+      if (k == 0) return expf(-psaz * vg.dhs[0] * p.absdry);
       const float cl = (k >= icltop && k < KX - 1) ? acloud : 0.0f;
-      W0[k] = expf(-psaz * vg.dhs[k] * (D.abs1[k] + p.abswv1 * Q[k] + cl));
-    }
+      return expf(-psaz * vg.dhs[k] * (D.abs1[k] + p.abswv1 * Q[k] + cl));
+    };
+    auto add_sw = [&](int k, float d) { DT[k] = DT[k] + (gate ? d * vg.grdscp[k] * rps : 0.0f); };
 #pragma unroll 4
-    for (int k = 0; k < KX - 1; ++k) W1[k] = ((S >> k) & 1u) ? refl : 0.0f;
-    W1[KX - 1] = p.albcls * clstr;
+    for (int k = 0; k < KX - 1; ++k) W[k] = ((S >> k) & 1u) ? refl : 0.0f;
+    W[KX - 1] = p.albcls * clstr;
     const float fband2 = 0.05f, fband1 = 0.95f;
     float f1 = z.fsol * fband1;
     float d0 = f1;
-    f1 = W0[0] * (f1 - z.ozupp * psa);
-    W2[0] = d0 + (-f1);
+    f1 = tau0_at(0) * (f1 - z.ozupp * psa);
+    add_sw(0, d0 + (-f1));
     d0 = f1;
-    f1 = W0[1] * (f1 - z.ozone * psa);
-    W2[1] = d0 + (-f1);
-#pragma unroll 1
-    for (int k = 2; k < KX; ++k) {
-      const float prev = f1, r = W1[k], t0 = W0[k];
-      f1 = prev * t0 * (1.0f - r);
-      W2[k] = prev * (1.0f - r) * (1.0f - t0);
-      W1[k] = r * prev;
-    }
+    f1 = tau0_at(1) * (f1 - z.ozone * psa);
+    const float d1_band1 = d0 + (-f1);
     float f2 = z.fsol * fband2;
-#pragma unroll 2
-    for (int k = 1; k < KX; ++k) {
-      const float tau1 = expf(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
+    {  // band 2 at level 1 completes level 1's downward absorption
+      const float tau1 = expf(-psaz * vg.dhs[1] * p.abswv2 * Q[1]);
       const float prev = f2;
       f2 = prev * tau1;
-      W2[k] = W2[k] + prev * (1.0f - tau1);
+      add_sw(1, d1_band1);
+      add_sw(1, prev * (1.0f - tau1));
+    }
+#pragma unroll 1
+    for (int k = 2; k < KX; ++k) {
+      const float prev = f1, r = W[k], t0 = tau0_at(k);
+      f1 = prev * t0 * (1.0f - r);
+      const float d = prev * (1.0f - r) * (1.0f - t0);
+      W[k] = r * prev;
+      const float tau1 = expf(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
+      const float prev2 = f2;
+      f2 = prev2 * tau1;
+      add_sw(k, d);
+      add_sw(k, prev2 * (1.0f - tau1));
     }
     rsds = f1 + f2;
     float up = f1 * albsfc;
     o.rsns = rsds - up;
-    const bool gate = (K.model_step % 3) == 0;
-    {
-      const float dlast = W2[KX - 1] + up * (1.0f - W0[KX - 1]);
-      DT[KX - 1] = DT[KX - 1] + (gate ? dlast * vg.grdscp[KX - 1] * rps : 0.0f);
-    }
+    float t_k = tau0_at(KX - 1);
+    add_sw(KX - 1, up * (1.0f - t_k));
 #pragma unroll 1
     for (int k = KX - 1; k >= 1; --k) {
-      up = up * W0[k] + W1[k];
-      const float d = W2[k - 1] + up * (1.0f - W0[k - 1]);
-      DT[k - 1] = DT[k - 1] + (gate ? d * vg.grdscp[k - 1] * rps : 0.0f);
+      up = up * t_k + W[k];
+      t_k = tau0_at(k - 1);
+      add_sw(k - 1, up * (1.0f - t_k));
     }
-    const float ftop_up = W0[0] * up + W1[0];
+    const float ftop_up = t_k * up + W[0];
     o.ftop_sw = z.fsol - ftop_up;
     flux_sw0 = ftop_up;
     flux_sw1 = f2;
   }
   o.rsds = rsds;
 
-  // ---- longwave transmissivities (shortwave_radiation.py:174-206): W0..W3 = tau per band ---
-  {
-    const float acl1 = cloudc * p.ablcl1, acl2 = cloudc * p.ablcl2;
-#pragma unroll 2
-    for (int k = 0; k < KX; ++k) {
-      const float qk = Q[k];
-      float a0 = p.ablwin, a2 = p.ablwv1 * qk, a3 = p.ablwv2 * qk;
-      if (k == 0) {
-        a2 = 0.0f;
-        a3 = 0.0f;
-      }
-      if (k >= 2 && k <= KX - 2) {
-        a0 = a0 + ((k > icltop) ? acl1 : acl2);
-        a2 = fmaxf(a2, acl2);
-        a3 = fmaxf(a3, acl2);
-      }
-      W0[k] = expf(-a0 * psa * vg.dhs[k]);
-      W1[k] = expf(-D.ablco2 * psa * vg.dhs[k]);
-      W2[k] = expf(-a2 * psa * vg.dhs[k]);
-      W3[k] = expf(-a3 * psa * vg.dhs[k]);
+  // ---- longwave transmissivities of level k (shortwave_radiation.py:174-206) ---------------
+  const float acl1 = cloudc * p.ablcl1, acl2 = cloudc * p.ablcl2;
+  auto lw_tau = [&](int k, float tau[4]) {
+    const float qk = Q[k];
+    float a0 = p.ablwin, a2 = p.ablwv1 * qk, a3 = p.ablwv2 * qk;
+    if (k == 0) {
+      a2 = 0.0f;
+      a3 = 0.0f;
     }
-  }
+    if (k >= 2 && k <= KX - 2) {
+      a0 = a0 + ((k > icltop) ? acl1 : acl2);
+      a2 = fmaxf(a2, acl2);
+      a3 = fmaxf(a3, acl2);
+    }
+    tau[0] = expf(-a0 * psa * vg.dhs[k]);
+    tau[1] = expf(-D.ablco2 * psa * vg.dhs[k]);
+    tau[2] = expf(-a2 * psa * vg.dhs[k]);
+    tau[3] = expf(-a3 * psa * vg.dhs[k]);
+  };
+  auto add_lw = [&](int k, float d) { DT[k] = DT[k] + d * vg.grdscp[k] * rps; };
 
-  // ---- get_downward_longwave_rad_fluxes (longwave_radiation.py:13-117): W4 = dfabs --------
+  // ---- get_downward_longwave_rad_fluxes (longwave_radiation.py:13-117) ---------------------
   float rlds;
   {
-    float fl[4], fb[4], s0, s1;
+    float fl[4], fb[4], tau[4], s0, s1;
     st4a_at<KX>(K, T, 0, s0, s1);
     radset_w(T[0], D.w_lw, fb);
-    const float tz[4] = {W0[0], W1[0], W2[0], W3[0]};
+    lw_tau(0, tau);
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      const float emis = 1.0f - tz[b];
+      const float emis = 1.0f - tau[b];
       fl[b] = emis * (fb[b] * (s0 + emis * s1));
     }
     fl[2] = 0.0f;
     fl[3] = 0.0f;
     float sprev = sum4(fl);
-    W4[0] = 0.0f + (-sprev);
+    add_lw(0, 0.0f + (-sprev));
 #pragma unroll 1
     for (int k = 1; k < KX; ++k) {
       st4a_at<KX>(K, T, k, s0, s1);
       radset_w(T[k], D.w_lw, fb);
-      const float tk[4] = {W0[k], W1[k], W2[k], W3[k]};
+      lw_tau(k, tau);
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        const float emis = 1.0f - tk[b];
-        fl[b] = tk[b] * fl[b] + emis * (fb[b] * (s0 + emis * s1));
+        const float emis = 1.0f - tau[b];
+        fl[b] = tau[b] * fl[b] + emis * (fb[b] * (s0 + emis * s1));
       }
       const float sk = sum4(fl);
-      W4[k] = 0.0f + (-(sk - sprev));
+      float d = 0.0f + (-(sk - sprev));
+      if (k == KX - 1) d = d + (-(D.corlw_f * s0));
+      add_lw(k, d);
       sprev = sk;
     }
     const float ef[4] = {p.emisfc * fl[0], p.emisfc * fl[1], p.emisfc * fl[2], p.emisfc * fl[3]};
     rlds = sum4(ef);
-    st4a_at<KX>(K, T, KX - 1, s0, s1);
-    const float corlw = D.corlw_f * s0;
-    W4[KX - 1] = W4[KX - 1] + (-corlw);
-    rlds = rlds + corlw;
+    rlds = rlds + D.corlw_f * s0;
   }
   o.rlds = rlds;
 
@@ -452,7 +459,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
       vstr0 = -cdldv * va;
       shf0 = D.chlcp * denv1 * (tskin - t1_0);
       const float q1_0 = (p.fhum0 > 0.0f)
-                             ? p.fhum0 * (RH[KX - 1] * qsat_of(t1_0, psa, 1.0f)) + D.ghum0 * q_b
+                             ? p.fhum0 * (rh_at(KX - 1) * qsat_of(t1_0, psa, 1.0f)) + D.ghum0 * q_b
                              : q_b;
       const float qs00 = qsat_of(tskin, psa, 1.0f);
       evap0 = p.chl * denv1 * fmaxf(0.0f, s.soilw * qs00 - q1_0);
@@ -476,7 +483,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
                                       : fmaxf(-p.dtheta, D.astab * (sst - t2_1));
       denv2 = denv0 * (1.0f + dths * D.rdth);
       q1_1 = (p.fhum0 > 0.0f)
-                 ? p.fhum0 * (RH[KX - 1] * qsat_of(t1_1, psa, 1.0f)) + D.ghum0 * q_b
+                 ? p.fhum0 * (rh_at(KX - 1) * qsat_of(t1_1, psa, 1.0f)) + D.ghum0 * q_b
                  : q_b;
       const float cdsdv = p.cds * denv2;
       ustr1 = -cdsdv * ua;
@@ -510,114 +517,110 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
   // ---- get_upward_longwave_rad_fluxes (longwave_radiation.py:119-202) ---------------------
   {
     o.rlns = rlus2 - rlds;
-    float fb[4], fl[4], s0, s1;
+    float fb[4], fl[4], tau[4], s0, s1;
     radset_w(tsfc, D.w_lw, fb);
     const float fsw[4] = {flux_sw0, flux_sw1, 0.0f, 0.0f};
 #pragma unroll
     for (int b = 0; b < 4; ++b) fl[b] = fb[b] * rlus2 + D.refsfc * fsw[b];
-    W4[KX - 1] = W4[KX - 1] + p.epslw * rlus2;
     float sk = sum4(fl);
+    float d_last = p.epslw * rlus2;  // dfabs[kx-1] += epslw*rlus before the scan
 #pragma unroll 1
     for (int k = KX - 1; k >= 1; --k) {
       st4a_at<KX>(K, T, k, s0, s1);
       radset_w(T[k], D.w_lw, fb);
-      const float tk[4] = {W0[k], W1[k], W2[k], W3[k]};
+      lw_tau(k, tau);
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        const float emis = 1.0f - tk[b];
-        fl[b] = tk[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1));
+        const float emis = 1.0f - tau[b];
+        fl[b] = tau[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1));
       }
       const float skm1 = sum4(fl);
-      const float d = W4[k] + (sk - skm1);
-      if (k >= 2) DT[k] = DT[k] + d * vg.grdscp[k] * rps;
-      else W4[k] = d;
+      float d = (sk - skm1);
+      if (k == KX - 1) d = d_last + d;
+      if (k >= 2) add_lw(k, d);
+      else d_last = d;  // level 1 still gets -corlw2
       sk = skm1;
     }
     st4a_at<KX>(K, T, 0, s0, s1);
     float s0b, s1b;
     st4a_at<KX>(K, T, 1, s0b, s1b);
     radset_w(T[0], D.w_lw, fb);
-    const float tz[4] = {W0[0], W1[0], W2[0], W3[0]};
+    lw_tau(0, tau);
     float top[4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      const float emis = 1.0f - tz[b];
-      top[b] = (b < 2) ? tz[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1)) : fl[b];
+      const float emis = 1.0f - tau[b];
+      top[b] = (b < 2) ? tau[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1)) : fl[b];
     }
-    float d0 = W4[0] + ((fl[0] - top[0]) + (fl[1] - top[1]));
     const float stratc0 = z.stratz * psa, stratc1 = D.eps1 * psa;
     const float corlw1 = vg.dhs[0] * stratc1 * s0 + stratc0;
     const float corlw2 = vg.dhs[1] * stratc1 * s0b;
-    d0 = d0 + (-corlw1);
-    const float d1 = W4[1] + (-corlw2);
-    DT[0] = DT[0] + d0 * vg.grdscp[0] * rps;
-    DT[1] = DT[1] + d1 * vg.grdscp[1] * rps;
+    add_lw(0, ((fl[0] - top[0]) + (fl[1] - top[1])) + (-corlw1));
+    add_lw(1, d_last + (-corlw2));
     o.ftop_lw = (corlw1 + corlw2) + sum4(top);
   }
 
-  // ---- get_vertical_diffusion_tend (vertical_diffusion.py:10-136): W0 = tt, W1 = qt --------
+  // ---- get_vertical_diffusion_tend (vertical_diffusion.py:10-136) -------------------------
+  // Each level's ttenvd / qtenvd is formed completely, in the reference's order, and then added
+  // to the accumulated tendency (total + ttenvd, speedy_physics.py:125).  The "-" updates of
+  // lines 118 and 131 reach level k one step after its "+" update, so one ascending pass
+  // carries them in a register.
   {
     const int nl1 = KX - 1;
     const int icnv = KX - iptop - 1;
-#pragma unroll 4
-    for (int k = 0; k < KX; ++k) {
-      W0[k] = 0.0f;
-      W1[k] = 0.0f;
-    }
+    const float rh_b = rh_at(KX - 1), rh_b1 = rh_at(nl1 - 1);
     const float dmse = se_b - se_b1 + kAlhc * (q_b - QS[nl1 - 1]);
-    const float drh = RH[KX - 1] - RH[nl1 - 1];
+    const float drh = rh_b - rh_b1;
     const float fcnv = (icnv > 0 && dmse >= 0.0f) ? p.redshc : 1.0f;
+    float tt_sh1 = 0.0f, tt_sh0 = 0.0f, qt_sh1 = 0.0f, qt_sh0 = 0.0f;  // levels kx-2, kx-1
     if (dmse >= 0.0f) {
       const float fluxse = fcnv * D.fshcse * dmse;
-      W0[nl1 - 1] = fluxse * D.rsig[nl1 - 1];
-      W0[KX - 1] = -fluxse * D.rsig[KX - 1];
+      tt_sh1 = fluxse * D.rsig[nl1 - 1];
+      tt_sh0 = -fluxse * D.rsig[KX - 1];
       if (drh >= 0.0f) {
         const float fq = fcnv * D.fshcq * QS[KX - 1] * drh;
-        W1[nl1 - 1] = fq * D.rsig[nl1 - 1];
-        W1[KX - 1] = -fq * D.rsig[KX - 1];
+        qt_sh1 = fq * D.rsig[nl1 - 1];
+        qt_sh0 = -fq * D.rsig[KX - 1];
       }
     } else if (dmse < 0.0f && drh > D.drh0) {
       const float fq = D.fvdiq2 * QS[nl1 - 1] * drh;
-      W1[nl1 - 1] = fq * D.rsig[nl1 - 1];
-      W1[KX - 1] = -fq * D.rsig[KX - 1];
+      qt_sh1 = fq * D.rsig[nl1 - 1];
+      qt_sh0 = -fq * D.rsig[KX - 1];
     }
-    // moisture diffusion above the PBL: the "+" updates of all levels first, then the "-"
-    float rh_k = RH[2];
+    // moisture diffusion above the PBL (lines 99-118), levels 2..kx-3 and the "-" at kx-2
+    float pend = 0.0f;
+    float rh_k = rh_at(2);
 #pragma unroll 1
     for (int k = 2; k < KX - 2; ++k) {
-      const float rh_n = RH[k + 1];
+      const float rh_n = rh_at(k + 1);
       const float dr = rh_n - rh_k;
       const bool cond = (D.vdcond >> k) & 1u;
       const float fq = (dr >= D.drh0v[k] && cond) ? D.fvdiq2v[k] * QS[k] * dr : 0.0f;
-      W1[k] = W1[k] + fq * D.rsig[k];
-      W2[k] = fq;
+      const float qk = (k == 2) ? (0.0f + fq * D.rsig[k]) : (0.0f + fq * D.rsig[k]) + pend;
+      DQ[k] = DQ[k] + qk;
+      pend = -fq * D.rsig[k + 1];
       rh_k = rh_n;
     }
-#pragma unroll 1
-    for (int k = 2; k < KX - 2; ++k) W1[k + 1] = W1[k + 1] + (-W2[k] * D.rsig[k + 1]);
-    // damping of super-adiabatic lapse rate: "+" updates first, then the cumulative "-"
+    DQ[KX - 2] = DQ[KX - 2] + (qt_sh1 + pend);
+    DQ[KX - 1] = DQ[KX - 1] + qt_sh0;
+    // damping of super-adiabatic lapse rate (lines 121-131)
+    float cum = 0.0f;
     float se_k = se_at(T, PHI, 0), phi_k = PHI[0];
+    float pend_t = 0.0f;
 #pragma unroll 1
     for (int k = 0; k < nl1; ++k) {
       const float se_n = se_at(T, PHI, k + 1), phi_n = PHI[k + 1];
       const float se0 = se_n - p.segrad * (phi_n - phi_k);
       const float fse = (se_k < se0) ? D.fvdise * (se0 - se_k) : 0.0f;
-      W0[k] = W0[k] + fse * D.rsig[k];
-      W2[k] = fse;
+      const float base = (k == KX - 2) ? tt_sh1 : 0.0f;
+      const float tk = (k == 0) ? (base + fse * D.rsig[k]) : (base + fse * D.rsig[k]) + pend_t;
+      DT[k] = DT[k] + tk;
+      cum = cum + fse * D.rsig1[k];
+      pend_t = -cum;
       se_k = se_n;
       phi_k = phi_n;
     }
-    float cum = 0.0f;
-#pragma unroll 1
-    for (int k = 0; k < nl1; ++k) {
-      cum = cum + W2[k] * D.rsig1[k];
-      W0[k + 1] = W0[k + 1] + (-cum);
-    }
-#pragma unroll 4
-    for (int k = 0; k < KX; ++k) {
-      DT[k] = DT[k] + W0[k];
-      DQ[k] = DQ[k] + W1[k];
-    }
+    DT[KX - 1] = DT[KX - 1] + (tt_sh0 + pend_t);
   }
 }
 

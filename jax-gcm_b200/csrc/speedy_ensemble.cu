@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kBlock) ensemble_prepass(const __grid_constant
   }
 }
 
-__global__ void __launch_bounds__(kNT, 2) ensemble_columns(const __grid_constant__ ClassArgs A,
+__global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant__ ClassArgs A,
                                                            const MemberDev* __restrict__ members,
                                                            const Tile* __restrict__ tiles,
                                                            int ntiles) {
