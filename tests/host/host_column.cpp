@@ -1,0 +1,146 @@
+// Host build of the generic column physics (jax-gcm_b200/csrc/speedy_generic.h) for the CPU
+// tests: forward in float32 and float64, and the reverse-mode VJP in float64 with the tape in
+// host memory.  Test infrastructure only.
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "speedy_generic.h"
+
+using spdad::Adj;
+using spdad::TapeT;
+
+struct HostColumn {
+  int kx;
+  uint32_t flags;
+  int model_step;
+  float ablco2;
+  uint32_t S;
+  float t[16], q[16], phi[16];
+  float psa, u_low, v_low;
+  float sst, stl, soilw, snowc, sice, alb0, fmask, orog, phis0;
+  float fsol, ozupp, ozone, zenit, stratz, sqrt_coa;
+};
+
+struct HostOut {
+  double dt[16], dq[16], du_low, dv_low, precnv, precls, cloudc, rsds, rlds;
+  int iptop, icltop;
+};
+
+template <class R, class F>
+static void fill_in(const HostColumn& h, spdgen::ColumnIn<R, F>& in) {
+  for (int k = 0; k < h.kx; ++k) {
+    in.t[k] = R(F(h.t[k]));
+    in.q[k] = R(F(h.q[k]));
+    in.phi[k] = R(F(h.phi[k]));
+  }
+  in.psa = R(F(h.psa));
+  in.u_low = R(F(h.u_low));
+  in.v_low = R(F(h.v_low));
+  in.sst = h.sst; in.stl = h.stl; in.soilw = h.soilw; in.snowc = h.snowc; in.sice = h.sice;
+  in.alb0 = h.alb0; in.fmask = h.fmask; in.orog = h.orog; in.phis0 = h.phis0;
+  in.fsol = h.fsol; in.ozupp = h.ozupp; in.ozone = h.ozone; in.zenit = h.zenit;
+  in.stratz = h.stratz; in.sqrt_coa = h.sqrt_coa;
+}
+
+template <class R>
+static void fill_params(const spd_params_t& p, spdgen::DiffParams<R>& g) {
+  g.psmin = R(p.psmin); g.trcnv = R(p.trcnv); g.rhil = R(p.rhil); g.rhbl = R(p.rhbl);
+  g.entmax = R(p.entmax); g.smf = R(p.smf); g.trlsc = R(p.trlsc); g.rhlsc = R(p.rhlsc);
+  g.drhlsc = R(p.drhlsc); g.rhblsc = R(p.rhblsc); g.albcl = R(p.albcl); g.albcls = R(p.albcls);
+}
+
+template <int KX, class F>
+static void fwd(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h, HostOut& out) {
+  spdgen::ColumnIn<F, F> in;
+  fill_in(h, in);
+  spdgen::DiffParams<F> g;
+  fill_params(p, g);
+  spdgen::ColumnOut<F> o;
+  spdgen::column_generic<KX, F, F>(vg, p, g, h.flags, h.model_step, F(h.ablco2), h.S, in, o);
+  for (int k = 0; k < KX; ++k) {
+    out.dt[k] = o.dt[k];
+    out.dq[k] = o.dq[k];
+  }
+  out.du_low = o.du_low; out.dv_low = o.dv_low; out.precnv = o.precnv; out.precls = o.precls;
+  out.cloudc = o.cloudc; out.rsds = o.rsds; out.rlds = o.rlds;
+  out.iptop = o.iptop; out.icltop = o.icltop;
+}
+
+// VJP in float64: ct_dt/ct_dq [kx], ct_du/ct_dv (lowest level).  Gradients: g_t, g_q, g_phi
+// [kx], g_psa, g_u, g_v (lowest level), g_params[12].  Returns the tape length.
+template <int KX>
+static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h,
+               const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv,
+               double* g_t, double* g_q, double* g_phi, double* g_psa, double* g_u,
+               double* g_v, double* g_params) {
+  typedef Adj<double> A;
+  const int cap = 1 << 20;
+  std::vector<int32_t> ia(cap), ib(cap);
+  std::vector<double> pa(cap), pb(cap), adj(cap);
+  TapeT<double> tp{ia.data(), ib.data(), pa.data(), pb.data(), adj.data(), 1, 0, cap, 0};
+  auto leaf = [&](double v) { return A(v, tp.leaf(), &tp); };
+  spdgen::DiffParams<A> g;
+  g.psmin = leaf(p.psmin); g.trcnv = leaf(p.trcnv); g.rhil = leaf(p.rhil); g.rhbl = leaf(p.rhbl);
+  g.entmax = leaf(p.entmax); g.smf = leaf(p.smf); g.trlsc = leaf(p.trlsc);
+  g.rhlsc = leaf(p.rhlsc); g.drhlsc = leaf(p.drhlsc); g.rhblsc = leaf(p.rhblsc);
+  g.albcl = leaf(p.albcl); g.albcls = leaf(p.albcls);
+  spdgen::ColumnIn<A, double> in;
+  fill_in(h, in);
+  for (int k = 0; k < KX; ++k) {
+    in.t[k] = leaf(h.t[k]);
+    in.q[k] = leaf(h.q[k]);
+    in.phi[k] = leaf(h.phi[k]);
+  }
+  in.psa = leaf(h.psa);
+  in.u_low = leaf(h.u_low);
+  in.v_low = leaf(h.v_low);
+  spdgen::ColumnOut<A> o;
+  spdgen::column_generic<KX, A, double>(vg, p, g, h.flags, h.model_step, double(h.ablco2), h.S,
+                                        in, o);
+  for (int k = 0; k < KX; ++k) {
+    tp.seed(o.dt[k].i, ct_dt[k]);
+    tp.seed(o.dq[k].i, ct_dq[k]);
+  }
+  tp.seed(o.du_low.i, ct_du);
+  tp.seed(o.dv_low.i, ct_dv);
+  tp.reverse();
+  for (int k = 0; k < KX; ++k) {
+    g_t[k] = tp.grad(in.t[k].i);
+    g_q[k] = tp.grad(in.q[k].i);
+    g_phi[k] = tp.grad(in.phi[k].i);
+  }
+  *g_psa = tp.grad(in.psa.i);
+  *g_u = tp.grad(in.u_low.i);
+  *g_v = tp.grad(in.v_low.i);
+  const A* ps[12] = {&g.psmin, &g.trcnv, &g.rhil, &g.rhbl, &g.entmax, &g.smf,
+                     &g.trlsc, &g.rhlsc, &g.drhlsc, &g.rhblsc, &g.albcl, &g.albcls};
+  for (int j = 0; j < 12; ++j) g_params[j] = tp.grad(ps[j]->i);
+  return tp.overflow ? -1 : tp.n;
+}
+
+extern "C" {
+
+int hc_fwd(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h, int f64,
+           HostOut* out) {
+  switch (h->kx) {
+    case 7: f64 ? fwd<7, double>(*vg, *p, *h, *out) : fwd<7, float>(*vg, *p, *h, *out); return 0;
+    case 8: f64 ? fwd<8, double>(*vg, *p, *h, *out) : fwd<8, float>(*vg, *p, *h, *out); return 0;
+    case 16: f64 ? fwd<16, double>(*vg, *p, *h, *out) : fwd<16, float>(*vg, *p, *h, *out); return 0;
+  }
+  return -1;
+}
+
+int hc_vjp(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h,
+           const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv, double* g_t,
+           double* g_q, double* g_phi, double* g_psa, double* g_u, double* g_v,
+           double* g_params) {
+  switch (h->kx) {
+    case 7: return vjp<7>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+    case 8: return vjp<8>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+    case 16: return vjp<16>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+  }
+  return -2;
+}
+
+}  // extern "C"
