@@ -131,6 +131,39 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
             size_t scratch_bytes, void* stream);
 
 /* ----------------------------------------------------------------------------------------- */
+/* Adjoint (vector-Jacobian product) of the plain forward.                                    */
+/* Replaces jax.vjp of SpeedyPhysics.compute_tendencies (speedy_physics.py:88-127; the         */
+/* reference differentiates through jax.checkpoint-ed terms, speedy_physics.py:82-86).         */
+/* Each thread re-evaluates its column's forward recording a reverse-mode tape in `scratch`    */
+/* (recompute in column, nothing stored from the forward call) and sweeps it backwards.        */
+/* Ties of min/max split the derivative 0.5/0.5 (JAX's lax.min/lax.max rule); integer levels  */
+/* and the instance level set carry no derivative.                                            */
+/* ----------------------------------------------------------------------------------------- */
+#define SPD_VJP_MAX_THREADS 32768
+#define SPD_NUM_DIFF_PARAMS 12
+
+/* Cotangents of the four tendency planes [kx][C]. */
+typedef struct {
+  const float *u_wind, *v_wind, *temperature, *specific_humidity;
+} spd_cotangents_t;
+
+/* Gradients with respect to the PhysicsState planes [kx][C] (u_wind and v_wind are nonzero only
+ * at the lowest level, the only level the physics reads), psa [C], and the 12 differentiated
+ * parameters in the order psmin, trcnv, rhil, rhbl, entmax, smf, trlsc, rhlsc, drhlsc, rhblsc,
+ * albcl, albcls (params.py:11-16, :51-54, :72-73), summed over columns. */
+typedef struct {
+  float *u_wind, *v_wind, *temperature, *specific_humidity, *geopotential;
+  float *normalized_surface_pressure;
+  float *params;
+} spd_grads_t;
+
+size_t spd_vjp_scratch_bytes(const spd_desc_t* desc);
+
+int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+            const spd_inputs_t* in, const spd_cotangents_t* ct, const spd_grads_t* grads,
+            void* scratch, size_t scratch_bytes, void* stream);
+
+/* ----------------------------------------------------------------------------------------- */
 /* Batched ragged ensemble: many instances ("members") of mixed resolution and level count,  */
 /* e.g. a forecast ensemble or a set of independent grids, in one pair of persistent launches  */
 /* (cloud-top pre-pass over every member, then the column pass over every member).  Each      */

@@ -84,6 +84,20 @@ class PlanInfo(C.Structure):
 
 MAX_CLASSES = 4
 
+
+class Cotangents(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("u_wind", "v_wind", "temperature", "specific_humidity")]
+
+
+class Grads(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("u_wind", "v_wind", "temperature", "specific_humidity",
+                                          "geopotential", "normalized_surface_pressure",
+                                          "params")]
+
+
+DIFF_PARAM_NAMES = ["psmin", "trcnv", "rhil", "rhbl", "entmax", "smf", "trlsc", "rhlsc",
+                    "drhlsc", "rhblsc", "albcl", "albcls"]
+
 STATUS = {0: "ok", 1: "null pointer", 2: "bad shape", 3: "unsupported kx", 4: "bad scratch",
           5: "CUDA error", 6: "device error status", 7: "misaligned pointer",
           8: "il above the no-allocation entry point's limit"}
@@ -121,6 +135,11 @@ def _declare(lib):
     lib.spd_ensemble_fwd.argtypes = [P(Class), C.c_int, C.c_void_p, P(PlanInfo), C.c_int,
                                      C.c_void_p]
     lib.spd_ensemble_fwd.restype = C.c_int
+    lib.spd_vjp_scratch_bytes.argtypes = [P(Desc)]
+    lib.spd_vjp_scratch_bytes.restype = C.c_size_t
+    lib.spd_vjp.argtypes = [P(Desc), P(VGrid), P(Params), P(Inputs), P(Cotangents), P(Grads),
+                            C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.spd_vjp.restype = C.c_int
     for name, spec in EXTRA_DECLS.items():
         fn = getattr(lib, name, None)
         if fn is not None:

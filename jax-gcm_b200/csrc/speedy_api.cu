@@ -16,16 +16,6 @@ namespace spd {
 constexpr size_t kHeaderBytes = 256;  // S word, status word, padding
 
 template <int KX>
-__global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const spd_inputs_t in,
-                                                           uint32_t* __restrict__ S,
-                                                           ZonalRow* __restrict__ table) {
-  const int c = blockIdx.x * kBlock + threadIdx.x;
-  if (c < K.il) table[c] = zonal_row(K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
-  const uint32_t bit = (c < K.C) ? prepass_column<KX>(K, in, c, K.C) : 0u;
-  or_level_set(bit, S);
-}
-
-template <int KX>
 __global__ void __launch_bounds__(kNT, 4) column_kernel(const ConstsD CD, const spd_inputs_t in,
                                                         const spd_outputs_t out,
                                                         const uint32_t* __restrict__ S,

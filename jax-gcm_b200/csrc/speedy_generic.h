@@ -16,6 +16,14 @@
 #include "speedy_ad.h"
 #include "speedy_b200.h"
 
+// The column loops stay rolled on the device: with Adj values the per-level arrays live in
+// local memory anyway, and unrolling only multiplies code size and compile time.
+#if defined(__CUDA_ARCH__)
+#define SPD_ROLL _Pragma("unroll 1")
+#else
+#define SPD_ROLL
+#endif
+
 namespace spdgen {
 
 using spdad::gexp;
@@ -79,9 +87,11 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   const R* q = in.q;
   const R* phi = in.phi;
   R qsat[KX], rh[KX], se[KX];
+  SPD_ROLL
   for (int k = 0; k < KX; ++k) o.dt[k] = o.dq[k] = R(F(0));
 
   // ---- spec_hum_to_rel_hum (humidity.py:16-51) ----
+  SPD_ROLL
   for (int k = 0; k < KX; ++k) {
     qsat[k] = qsat_g<R, F>(t[k], psa, F(vg.fsg[k]));
     rh[k] = q[k] / qsat[k];
@@ -99,13 +109,16 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   R qdif = R(F(0));
   {
     R mss[KX], mss2[KX];
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) mss[k] = se[k] + F(2501.0) * qsat[k];
     const R mse0 = se[KX - 1] + F(2501.0) * q[KX - 1];
     const R mse1 = gmin(mse0, se[KX - 2] + F(2501.0) * q[KX - 2]);
     const R mss0 = gmax(mse0, mss[KX - 1]);
+    SPD_ROLL
     for (int k = 0; k < KX - 1; ++k) mss2[k] = mss[k] + F(vg.wvi[k][1]) * (mss[k + 1] - mss[k]);
     mss2[KX - 1] = R(F(0));
     int ktop1 = KX, ktop2 = KX;
+    SPD_ROLL
     for (int k = KX - 4; k >= 2; --k) {
       if (val(mss0) > val(mss2[k])) ktop1 = k + 1;
       if (val(mse1) > val(mss2[k])) ktop2 = k + 1;
@@ -127,12 +140,14 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   {
     R entr[KX];
     R sentr = R(F(0));
+    SPD_ROLL
     for (int k = 1; k < KX - 1; ++k) {
       const R e = gmax(F(0), R(F(vg.fsg[k]) - F(0.5)));
       entr[k] = e * e;
       sentr = sentr + entr[k];
     }
     const R escale = g.entmax / sentr;
+    SPD_ROLL
     for (int k = 1; k < KX - 1; ++k) entr[k] = entr[k] * escale;
     const R fm0 = F(1e5) * F(vg.dhs[KX - 1]) / (F(9.81) * g.trcnv * F(3600.0));
     const R rdps = F(2.0) / (F(1.0) - g.psmin);
@@ -140,6 +155,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const R qmax = gmax(F(1.01) * q[KX - 1], qsat[KX - 1]);
     R sb3[KX], qb3[KX];
     sb3[0] = qb3[0] = R(F(0));
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) {
       sb3[k] = se[k - 1] + F(vg.wvi[k - 1][1]) * (se[k] - se[k - 1]);
       qb3[k] = q[k - 1] + F(vg.wvi[k - 1][1]) * (q[k] - q[k - 1]);
@@ -153,6 +169,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const R fds = fmass * sb, fdq = fmass * qb;
     R dfse[KX], dfqa[KX], fm3[KX], fus3[KX], fuq3[KX], fds3[KX], fdq3[KX];
     R cm = R(F(0)), cs = R(F(0)), cq = R(F(0));
+    SPD_ROLL
     for (int k = KX - 1; k >= 0; --k) {
       const bool lm = (k <= KX - 2) && (k >= iptop);
       R en = (k >= 1 && k <= KX - 2) ? entr[k] * psa * cbmf : R(F(0));
@@ -168,6 +185,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     }
     dfse[KX - 1] = fds - fus;
     dfqa[KX - 1] = fdq - fuq;
+    SPD_ROLL
     for (int k = 0; k < KX - 1; ++k) {
       const bool lm = (k >= iptop);
       const R a = (fus3[k + 1] - fds3[k + 1]) - (fus3[k] - fds3[k]);
@@ -176,6 +194,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       dfqa[k] = lm ? b : F(0) * b;
     }
     R fsq_sum = R(F(0));
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) {
       const bool lm = (k <= KX - 2) && (k >= iptop);
       const R d0 = g.rhil * qsat[k] - q[k];
@@ -195,6 +214,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const R rps = F(1) / psa;
     o.dt[0] = o.dt[0] + dfse[0];
     o.dq[0] = o.dq[0] + dfqa[0];
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) {
       o.dt[k] = o.dt[k] + dfse[k] * rps * F(vg.grdscp[k]);
       o.dq[k] = o.dq[k] + dfqa[k] * rps * F(vg.grdsig[k]);
@@ -211,6 +231,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const R psa2 = psa * psa;
     R psum = R(F(0));
     int first = 0;
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) {
       const F sig2 = F(vg.fsg[k]) * F(vg.fsg[k]);
       const R rhref = gmax(g.rhlsc + g.drhlsc * (sig2 - F(1.0)), g.rhblsc);
@@ -244,6 +265,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     bool mk[KX];
     R cmax = R(F(0));
     bool first = true;
+    SPD_ROLL
     for (int k = 2; k < KX - 2; ++k) {
       const R drh = rh[k] - F(p.rhcl1);
       mk[k] = val(drh) > val(cloudc0) && val(q[k]) > F(p.qacl);
@@ -252,6 +274,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       first = false;
     }
     int icl = -1;
+    SPD_ROLL
     for (int k = 2; k < KX - 2; ++k) {
       const int cand = (val(cmax) == val(upd[k])) ? (mk[k] ? k : icl0) : icl0;
       icl = cand > icl ? cand : icl;
@@ -278,11 +301,13 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   {
     const bool cmask = icltop < KX;
     R tau0[KX], tau1[KX], r[KX], dfabs[KX];
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) r[k] = ((S >> k) & 1u) && cmask ? g.albcl * cloudc : R(F(0));
     r[KX - 1] = g.albcls * clstr;
     const R psaz = psa * in.zenit;
     const R acloud = cloudc * gmin(F(p.abscl1) * qcloud, F(p.abscl2));
     tau0[0] = gexp(-psaz * F(vg.dhs[0]) * F(p.absdry));
+    SPD_ROLL
     for (int k = 1; k < KX - 1; ++k) {
       const F abs1 = F(p.absdry) + F(p.absaer) * (F(vg.fsg[k]) * F(vg.fsg[k]));
       const R cl = (k >= icltop) ? acloud : F(0) * acloud;
@@ -292,6 +317,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       const F abs1 = F(p.absdry) + F(p.absaer) * (F(vg.fsg[KX - 1]) * F(vg.fsg[KX - 1]));
       tau0[KX - 1] = gexp(-psaz * F(vg.dhs[KX - 1]) * (abs1 + F(p.abswv1) * q[KX - 1]));
     }
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) tau1[k] = gexp(-psaz * F(vg.dhs[k]) * F(p.abswv2) * q[k]);
     R f1 = in.fsol * F(0.95);
     dfabs[0] = f1;
@@ -300,6 +326,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     dfabs[1] = f1;
     f1 = tau0[1] * (f1 - in.ozone * psa);
     dfabs[1] = dfabs[1] + (-f1);
+    SPD_ROLL
     for (int k = 2; k < KX; ++k) {
       const R prev = f1;
       f1 = prev * tau0[k] * (F(1) - r[k]);
@@ -307,6 +334,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       r[k] = r[k] * prev;
     }
     R f2 = R(in.fsol * F(0.05));
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) {
       const R prev = f2;
       f2 = prev * tau1[k];
@@ -315,6 +343,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     rsds = f1 + f2;
     R up = f1 * albsfc;
     dfabs[KX - 1] = dfabs[KX - 1] + up * (F(1) - tau0[KX - 1]);
+    SPD_ROLL
     for (int k = KX - 1; k >= 1; --k) {
       up = up * tau0[k] + r[k];
       dfabs[k - 1] = dfabs[k - 1] + up * (F(1) - tau0[k - 1]);
@@ -322,6 +351,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     flux_sw0 = tau0[0] * up + r[0];
     flux_sw1 = f2;
     if ((model_step % 3) == 0) {
+      SPD_ROLL
       for (int k = 0; k < KX; ++k) o.dt[k] = o.dt[k] + dfabs[k] * F(vg.grdscp[k]) / psa;
     }
   }
@@ -331,6 +361,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   R tau[KX][4], st0[KX], st1[KX], dfl[KX];
   {
     const R acl1 = cloudc * F(p.ablcl1), acl2 = cloudc * F(p.ablcl2);
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) {
       R a0 = R(F(p.ablwin)), a2 = F(p.ablwv1) * q[k], a3 = F(p.ablwv2) * q[k];
       if (k == 0) a2 = a3 = R(F(0));
@@ -345,6 +376,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       tau[k][3] = gexp(-a3 * psa * F(vg.dhs[k]));
     }
     R th[KX];
+    SPD_ROLL
     for (int k = 0; k < KX - 1; ++k) th[k] = t[k] + F(vg.wvi[k][1]) * (t[k + 1] - t[k]);
     const R s10 = F(0.75) * t[0] + F(0.25) * th[0];
     const R s11 = F(0.50) * t[1] + F(0.25) * (th[0] + th[1]);
@@ -353,6 +385,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     st1[0] = R(F(0));
     st0[1] = sbc * ((s11 * s11) * (s11 * s11));
     st1[1] = R(F(0));
+    SPD_ROLL
     for (int k = 2; k < KX; ++k) {
       const R grad = (k < KX - 1) ? F(0.5) * gmax(th[k] - th[k - 1], F(0.0))
                                   : gmax(t[KX - 1] - th[KX - 2], F(0.0));
@@ -365,6 +398,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   {
     R fl[4], fb[4];
     radset_r(t[0], F(p.epslw), fb);
+    SPD_ROLL
     for (int b = 0; b < 4; ++b) {
       const R emis = F(1) - tau[0][b];
       fl[b] = emis * (fb[b] * (st0[0] + emis * st1[0]));
@@ -372,8 +406,10 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     fl[2] = fl[3] = R(F(0));
     R sprev = ((fl[0] + fl[1]) + fl[2]) + fl[3];
     dfl[0] = F(0) + (-sprev);
+    SPD_ROLL
     for (int k = 1; k < KX; ++k) {
       radset_r(t[k], F(p.epslw), fb);
+      SPD_ROLL
       for (int b = 0; b < 4; ++b) {
         const R emis = F(1) - tau[k][b];
         fl[b] = tau[k][b] * fl[b] + emis * (fb[b] * (st0[k] + emis * st1[k]));
@@ -492,11 +528,14 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     R fb[4], fl[4];
     radset_r(R(tsfc), F(p.epslw), fb);
     const R fsw[4] = {flux_sw0, flux_sw1, R(F(0)), R(F(0))};
+    SPD_ROLL
     for (int b = 0; b < 4; ++b) fl[b] = fb[b] * rlus2 + refsfc * fsw[b];
     dfl[KX - 1] = dfl[KX - 1] + F(p.epslw) * rlus2;
     R sk = ((fl[0] + fl[1]) + fl[2]) + fl[3];
+    SPD_ROLL
     for (int k = KX - 1; k >= 1; --k) {
       radset_r(t[k], F(p.epslw), fb);
+      SPD_ROLL
       for (int b = 0; b < 4; ++b) {
         const R emis = F(1) - tau[k][b];
         fl[b] = tau[k][b] * fl[b] + emis * (fb[b] * (st0[k] - emis * st1[k]));
@@ -507,6 +546,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     }
     radset_r(t[0], F(p.epslw), fb);
     R top[4];
+    SPD_ROLL
     for (int b = 0; b < 4; ++b) {
       const R emis = F(1) - tau[0][b];
       top[b] = (b < 2) ? tau[0][b] * fl[b] + emis * (fb[b] * (st0[0] - emis * st1[0])) : fl[b];
@@ -518,6 +558,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const R corlw2 = F(vg.dhs[1]) * stratc1 * st0[1];
     dfl[0] = dfl[0] + (-corlw1);
     dfl[1] = dfl[1] + (-corlw2);
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) o.dt[k] = o.dt[k] + dfl[k] * F(vg.grdscp[k]) / psa;
   }
 
@@ -526,6 +567,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
     const int nl1 = KX - 1;
     const int icnv = KX - iptop - 1;
     R tt[KX], qt[KX];
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) tt[k] = qt[k] = R(F(0));
     const F cshc = F(vg.dhs[KX - 1]) / F(3600.0);
     const F cvdi = (F(vg.hsg[nl1]) - F(vg.hsg[1])) / (F(nl1 - 1) * F(3600.0));
@@ -551,6 +593,7 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       qt[KX - 1] = -fq * (F(1) / F(vg.dhs[KX - 1]));
     }
     R fluxq[KX];
+    SPD_ROLL
     for (int k = 2; k < KX - 2; ++k) {
       const bool cond = F(vg.hsg[k + 1]) > F(0.5);
       const F d0 = F(p.rhgrad) * (F(vg.fsg[k + 1]) - F(vg.fsg[k]));
@@ -559,18 +602,22 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
       fluxq[k] = (val(dr) >= d0 && cond) ? f2 * qsat[k] * dr : R(F(0));
       qt[k] = qt[k] + fluxq[k] * (F(1) / F(vg.dhs[k]));
     }
+    SPD_ROLL
     for (int k = 2; k < KX - 2; ++k) qt[k + 1] = qt[k + 1] + (-fluxq[k] * (F(1) / F(vg.dhs[k + 1])));
     R fse[KX];
+    SPD_ROLL
     for (int k = 0; k < nl1; ++k) {
       const R se0 = se[k + 1] - F(p.segrad) * (phi[k + 1] - phi[k]);
       fse[k] = (val(se[k]) < val(se0)) ? fvdise * (se0 - se[k]) : R(F(0));
       tt[k] = tt[k] + fse[k] * (F(1) / F(vg.dhs[k]));
     }
     R cum = R(F(0));
+    SPD_ROLL
     for (int k = 0; k < nl1; ++k) {
       cum = cum + fse[k] * (F(1) / (F(1) - F(vg.hsg[k + 1])));
       tt[k + 1] = tt[k + 1] + (-cum);
     }
+    SPD_ROLL
     for (int k = 0; k < KX; ++k) {
       o.dt[k] = o.dt[k] + tt[k];
       o.dq[k] = o.dq[k] + qt[k];

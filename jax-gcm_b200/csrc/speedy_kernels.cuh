@@ -133,4 +133,16 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   if (out.icltop) out.icltop[c] = o.icltop;
 }
 
+// Cloud-top pre-pass of one instance: the level set S (block OR, one atomic per block) and the
+// per-latitude solar table.
+template <int KX>
+__global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const spd_inputs_t in,
+                                                           uint32_t* __restrict__ S,
+                                                           ZonalRow* __restrict__ table) {
+  const int c = blockIdx.x * kBlock + threadIdx.x;
+  if (c < K.il) table[c] = zonal_row(K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
+  const uint32_t bit = (c < K.C) ? prepass_column<KX>(K, in, c, K.C) : 0u;
+  or_level_set(bit, S);
+}
+
 }  // namespace spd

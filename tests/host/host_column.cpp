@@ -69,23 +69,23 @@ static void fwd(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& 
 
 // VJP in float64: ct_dt/ct_dq [kx], ct_du/ct_dv (lowest level).  Gradients: g_t, g_q, g_phi
 // [kx], g_psa, g_u, g_v (lowest level), g_params[12].  Returns the tape length.
-template <int KX>
+template <int KX, class T = double>
 static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h,
                const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv,
                double* g_t, double* g_q, double* g_phi, double* g_psa, double* g_u,
                double* g_v, double* g_params) {
-  typedef Adj<double> A;
+  typedef Adj<T> A;
   const int cap = 1 << 20;
   std::vector<int32_t> ia(cap), ib(cap);
-  std::vector<double> pa(cap), pb(cap), adj(cap);
-  TapeT<double> tp{ia.data(), ib.data(), pa.data(), pb.data(), adj.data(), 1, 0, cap, 0};
-  auto leaf = [&](double v) { return A(v, tp.leaf(), &tp); };
+  std::vector<T> pa(cap), pb(cap), adj(cap);
+  TapeT<T> tp{ia.data(), ib.data(), pa.data(), pb.data(), adj.data(), 1, 0, cap, 0};
+  auto leaf = [&](T v) { return A(v, tp.leaf(), &tp); };
   spdgen::DiffParams<A> g;
   g.psmin = leaf(p.psmin); g.trcnv = leaf(p.trcnv); g.rhil = leaf(p.rhil); g.rhbl = leaf(p.rhbl);
   g.entmax = leaf(p.entmax); g.smf = leaf(p.smf); g.trlsc = leaf(p.trlsc);
   g.rhlsc = leaf(p.rhlsc); g.drhlsc = leaf(p.drhlsc); g.rhblsc = leaf(p.rhblsc);
   g.albcl = leaf(p.albcl); g.albcls = leaf(p.albcls);
-  spdgen::ColumnIn<A, double> in;
+  spdgen::ColumnIn<A, T> in;
   fill_in(h, in);
   for (int k = 0; k < KX; ++k) {
     in.t[k] = leaf(h.t[k]);
@@ -96,14 +96,13 @@ static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h
   in.u_low = leaf(h.u_low);
   in.v_low = leaf(h.v_low);
   spdgen::ColumnOut<A> o;
-  spdgen::column_generic<KX, A, double>(vg, p, g, h.flags, h.model_step, double(h.ablco2), h.S,
-                                        in, o);
+  spdgen::column_generic<KX, A, T>(vg, p, g, h.flags, h.model_step, T(h.ablco2), h.S, in, o);
   for (int k = 0; k < KX; ++k) {
-    tp.seed(o.dt[k].i, ct_dt[k]);
-    tp.seed(o.dq[k].i, ct_dq[k]);
+    tp.seed(o.dt[k].i, T(ct_dt[k]));
+    tp.seed(o.dq[k].i, T(ct_dq[k]));
   }
-  tp.seed(o.du_low.i, ct_du);
-  tp.seed(o.dv_low.i, ct_dv);
+  tp.seed(o.du_low.i, T(ct_du));
+  tp.seed(o.dv_low.i, T(ct_dv));
   tp.reverse();
   for (int k = 0; k < KX; ++k) {
     g_t[k] = tp.grad(in.t[k].i);
@@ -120,6 +119,18 @@ static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h
 }
 
 extern "C" {
+
+int hc_vjp32(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h,
+             const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv, double* g_t,
+             double* g_q, double* g_phi, double* g_psa, double* g_u, double* g_v,
+             double* g_params) {
+  switch (h->kx) {
+    case 7: return vjp<7, float>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+    case 8: return vjp<8, float>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+    case 16: return vjp<16, float>(*vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params);
+  }
+  return -2;
+}
 
 int hc_fwd(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h, int f64,
            HostOut* out) {

@@ -38,9 +38,8 @@ class HostOut(C.Structure):
                                           "rsds", "rlds")] + [("iptop", C.c_int), ("icltop", C.c_int)]
 
 
-@pytest.fixture(scope="module")
-def host(tmp_path_factory):
-    out = tmp_path_factory.mktemp("hostcol") / "libhostcol.so"
+def build_host(out):
+    """Compiles tests/host/host_column.cpp (g++) into ``out`` and declares its functions."""
     cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I" + os.path.join(ROOT, "include"),
            "-I" + os.path.join(ROOT, "jax-gcm_b200", "csrc"), "-o", str(out),
            os.path.join(ROOT, "tests", "host", "host_column.cpp")]
@@ -51,7 +50,13 @@ def host(tmp_path_factory):
     d = P(C.c_double)
     lib.hc_vjp.argtypes = [C.c_void_p, C.c_void_p, P(HostColumn), d, d, C.c_double,
                            C.c_double, d, d, d, d, d, d, d]
+    lib.hc_vjp32.argtypes = lib.hc_vjp.argtypes
     return lib
+
+
+@pytest.fixture(scope="module")
+def host(tmp_path_factory):
+    return build_host(tmp_path_factory.mktemp("hostcol") / "libhostcol.so")
 
 
 @pytest.fixture(scope="module")
@@ -142,12 +147,13 @@ def test_generic_forward_float64_matches_oracle_float64(pkg, host):
             assert abs(o.dt[k] - ref) <= tol * max(1e-4, np.max(np.abs(tend.temperature[:, i, j]))), k
 
 
-def _loss_and_grads(host, vg, pr, h, ct_t, ct_q, ct_u, ct_v):
+def _loss_and_grads(host, vg, pr, h, ct_t, ct_q, ct_u, ct_v, f32=False):
     kx = h.kx
     arr = lambda: (C.c_double * 16)()
     gt, gq, gphi, gp = arr(), arr(), arr(), (C.c_double * 12)()
     gpsa, gu, gv = C.c_double(), C.c_double(), C.c_double()
-    n = host.hc_vjp(C.byref(vg), C.byref(pr), C.byref(h), (C.c_double * 16)(*ct_t),
+    fn = host.hc_vjp32 if f32 else host.hc_vjp
+    n = fn(C.byref(vg), C.byref(pr), C.byref(h), (C.c_double * 16)(*ct_t),
                     (C.c_double * 16)(*ct_q), ct_u, ct_v, gt, gq, gphi, C.byref(gpsa),
                     C.byref(gu), C.byref(gv), gp)
     assert n > 0

@@ -1,0 +1,105 @@
+"""The GPU adjoint (spd_vjp) against the host build of the same generic column code, and
+autograd through the torch op.
+
+The host float64 VJP is the finite-difference-checked one (tests/test_adjoint_cpu.py); the
+GPU computes in float32.  Bar: for each gradient field, normwise |gpu - host64| <= 1e-4 of the
+field's max over the columns whose integer diagnostics agree, after allowing for float32
+noise of the same size as the host float32 VJP's own distance from float64.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from tests.test_adjoint_cpu import (HostOut, _flags, _loss_and_grads, build_host, column_of,
+                                    run_oracle, structs)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    return importlib.import_module("jax-gcm_b200")
+
+
+@pytest.fixture(scope="module")
+def host(tmp_path_factory):
+    return build_host(tmp_path_factory.mktemp("hostcol") / "libhostcol.so")
+
+
+def _gpu_vjp(pkg, inst, cts):
+    import torch
+    state, forcing, geom, date = pkg.instance_to_device(inst, "cuda")
+    phys = pkg.SpeedyPhysics(diagnostics=False)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float32, device="cuda")
+    cot = pkg.PhysicsTendency(t(cts["u"]), t(cts["v"]), t(cts["t"]), t(cts["q"]))
+    gs, gp = pkg.adjoint.vjp(phys, state, forcing, geom, date, cot)
+    torch.cuda.synchronize()
+    c = lambda x: x.cpu().numpy().astype(np.float64)
+    return dict(t=c(gs.temperature), q=c(gs.specific_humidity), phi=c(gs.geopotential),
+                psa=c(gs.normalized_surface_pressure), u=c(gs.u_wind), v=c(gs.v_wind)), c(gp)
+
+
+@pytest.mark.parametrize("kx", [8, 16])
+def test_gpu_vjp_matches_host(pkg, host, kx):
+    inst = pkg.synthetic.land_instance(700 + kx, 32, 16, kx)
+    tend, data, S = run_oracle(inst)
+    vg, pr = structs(pkg, inst)
+    rng = np.random.default_rng(kx)
+    shape = (kx, inst.ix, inst.il)
+    cts = dict(t=rng.normal(size=shape), q=rng.normal(size=shape), u=rng.normal(size=shape),
+               v=rng.normal(size=shape))
+    g_gpu, p_gpu = _gpu_vjp(pkg, inst, cts)
+    h64 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
+    h32 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
+    p64 = np.zeros(12)
+    for i in range(inst.ix):
+        for j in range(inst.il):
+            h = column_of(inst, data, S, i, j, _flags(inst))
+            ct = (list(cts["t"][:, i, j]) + [0.0] * (16 - kx),
+                  list(cts["q"][:, i, j]) + [0.0] * (16 - kx),
+                  float(cts["u"][-1, i, j]), float(cts["v"][-1, i, j]))
+            for f32, dst in ((False, h64), (True, h32)):
+                g, _ = _loss_and_grads(host, vg, pr, h, *ct, f32=f32)
+                dst["t"][:, i, j], dst["q"][:, i, j], dst["phi"][:, i, j] = g["t"], g["q"], g["phi"]
+                dst["psa"][i, j] = g["psa"]
+                dst["u"][-1, i, j], dst["v"][-1, i, j] = g["u"], g["v"]
+                if not f32:
+                    p64 += g["params"]
+    report = {}
+    for k in ("t", "q", "phi", "psa", "u", "v"):
+        scale = max(np.max(np.abs(h64[k])), 1e-30)
+        e_gpu = np.abs(g_gpu[k] - h64[k]) / scale
+        e_32 = np.abs(h32[k] - h64[k]) / scale
+        report[k] = (float(e_gpu.max()), float(e_32.max()))
+        # columns where float32 rounding flips a branch differ by O(1); allow a few
+        cols_bad = e_gpu.reshape(-1, inst.ix, inst.il).max(axis=0) > max(1e-4, 3 * e_32.max())
+        assert cols_bad.sum() <= max(2, 0.005 * inst.ix * inst.il), (k, report[k], cols_bad.sum())
+    print(inst.name, report)
+    rel = np.abs(p_gpu - p64) / np.maximum(np.abs(p64), 1e-30)
+    assert np.sum(rel > 1e-3) <= 1, (p_gpu, p64)
+
+
+def test_autograd_through_torch_op(pkg):
+    import torch
+    inst = pkg.synthetic.land_instance(55, 32, 16, 8)
+    state, forcing, geom, date = pkg.instance_to_device(inst, "cuda")
+    phys = pkg.SpeedyPhysics(diagnostics=False)
+    for f in ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential",
+              "normalized_surface_pressure"):
+        getattr(state, f).requires_grad_(True)
+    params = pkg.adjoint.parameter_vector(device="cpu").requires_grad_(True)
+    tend = pkg.adjoint.tendencies(phys, state, forcing, geom, date, params)
+    ref, _ = phys.compute_tendencies(pkg.PhysicsState(*(getattr(state, f).detach() for f in (
+        "u_wind", "v_wind", "temperature", "specific_humidity", "geopotential",
+        "normalized_surface_pressure"))), forcing, geom, date)
+    assert torch.equal(tend.temperature.detach(), ref.temperature)
+    w = torch.randn_like(tend.temperature)
+    loss = (tend.temperature * w).sum() + tend.specific_humidity.sum()
+    loss.backward()
+    cot = pkg.PhysicsTendency(torch.zeros_like(w), torch.zeros_like(w), w,
+                              torch.ones_like(w))
+    gs, gp = pkg.adjoint.vjp(phys, state, forcing, geom, date, cot)
+    assert torch.allclose(state.temperature.grad, gs.temperature)
+    assert torch.allclose(state.geopotential.grad, gs.geopotential)
+    assert torch.allclose(params.grad, gp.cpu())
