@@ -1,0 +1,772 @@
+"""Continuous-batching request loop for SPEEDY physics tendency and VJP requests.
+
+A request names 1..n members (grid instances, each a key into a member source) and asks either
+for their tendencies (``SpeedyPhysics.compute_tendencies``, jcm/physics/speedy/
+speedy_physics.py:88-127) or for the VJP of those tendencies (``jax.vjp`` of the same function)
+under a cotangent the request seeds.  The reference has no serving layer; this module is the
+layer a forecast service would put in front of the physics:
+
+* Admission by free HBM.  Every device byte the loop holds (resident member state, result and
+  cotangent buffers, the adjoint's scratch) is counted against ``budget_bytes``.  A request is
+  admitted, in arrival order, when its new members and its result buffers fit; idle resident
+  members are evicted least-recently-used to make room.  A request that can never fit is
+  rejected; a failed device allocation leaves the request waiting and is counted.
+* Device-resident column state.  A member's state, forcing and geometry are uploaded once, as
+  one packed buffer from pinned host memory on a copy stream, and stay on the device while any
+  request uses them (and afterwards, until evicted).
+* Continuous batching.  Tendency requests admitted while earlier batches run are merged into
+  the next batch: one ragged-ensemble launch pair (``spd_ensemble_fwd``) over all their members,
+  enqueued while up to ``max_inflight`` earlier batches are still on the device.  VJP requests
+  run on their own stream (``spd_vjp`` per member), so their work overlaps the tendency batches
+  on the device, and uploads overlap both.
+* Latency.  Completion times are device timestamps (CUDA events) mapped onto the host clock on
+  which arrivals are stamped; p50/p99 latency and columns/s are reported per run.
+
+``mode="plain"`` is the per-request drop-in on the same GPU: one request at a time in arrival
+order, every member through ``spd_fwd`` (or ``spd_vjp``) on one stream.
+
+The scheduler (``Scheduler``) is independent of the device; ``CudaBackend`` performs the device
+work through the C ABI.  Failures a caller can cause are handled on the host: malformed
+requests and requests larger than the budget are rejected at submission, allocation failures
+are retried, and ``cancel`` drops a waiting request or discards an in-flight one's results.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Dict, Hashable, List, Optional
+
+import numpy as np
+
+from . import _lib
+
+TENDENCY = "tendency"
+VJP = "vjp"
+KINDS = (TENDENCY, VJP)
+
+_ALIGN = 256
+
+# Instance attribute of each ABI input field (synthetic.Instance naming).
+_INSTANCE_FIELDS = dict(u_wind="u", v_wind="v", temperature="t", specific_humidity="q",
+                        geopotential="phi", normalized_surface_pressure="psa", alb0="alb0",
+                        sice_am="sice", snowc_am="snowc", soilw_am="soilw", stl_am="stl",
+                        sea_surface_temperature="sst", fmask="fmask", orog="orog",
+                        phis0="phis0", sia="sia", coa="coa")
+_LEVEL_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential")
+_LAT_FIELDS = ("sia", "coa")
+
+
+def _round_up(n, a=_ALIGN):
+    return (n + a - 1) // a * a
+
+
+def member_layout(kx, ix, il):
+    """Byte offsets of the 17 input fields in a member's packed buffer, and its size."""
+    c = ix * il
+    off, pos = {}, 0
+    for name in _lib.INPUT_FIELDS:
+        n = kx * c if name in _LEVEL_FIELDS else (il if name in _LAT_FIELDS else c)
+        off[name] = (pos, n)
+        pos = _round_up(pos + 4 * n)
+    return off, pos
+
+
+def tendency_result_floats(kx, ix, il):
+    """Floats of one member's tendency result: four tendency planes and two precipitation
+    fields."""
+    return (4 * kx + 2) * ix * il
+
+
+def vjp_result_floats(kx, ix, il):
+    """Floats of one member's VJP result and cotangent: gradients of u, v, T, q, phi and psa,
+    the 12 parameter gradients, and the four cotangent planes."""
+    return (5 * kx + 1) * ix * il + 12 + 4 * kx * ix * il
+
+
+@dataclass
+class HostMember:
+    """One member's inputs packed in one host buffer (pinned when torch can pin), in the
+    layout of ``member_layout``."""
+    kx: int
+    ix: int
+    il: int
+    lfluxland: bool
+    buffer: object          # torch uint8 tensor (CPU)
+    nbytes: int
+
+    @property
+    def columns(self):
+        return self.ix * self.il
+
+    @classmethod
+    def from_instance(cls, inst, pin=True):
+        import torch
+        off, nbytes = member_layout(inst.kx, inst.ix, inst.il)
+        buf = torch.zeros(nbytes, dtype=torch.uint8, pin_memory=pin and torch.cuda.is_available())
+        flat = buf.view(torch.float32) if nbytes % 4 == 0 else None
+        for name, (pos, n) in off.items():
+            a = np.ascontiguousarray(getattr(inst, _INSTANCE_FIELDS[name]), np.float32).ravel()
+            if a.size != n:
+                raise ValueError(f"field {name}: {a.size} values, expected {n}")
+            flat[pos // 4: pos // 4 + n] = torch.from_numpy(a)
+        return cls(inst.kx, inst.ix, inst.il, bool(inst.lfluxland), buf, nbytes)
+
+
+@dataclass
+class Request:
+    """A tendency or VJP request over ``members`` (keys of the member source)."""
+    kind: str
+    members: List[Hashable]
+    arrival: float = 0.0              # seconds after the stream's start
+    seed: int = 0                     # cotangent seed (VJP)
+    rid: int = -1
+    status: str = "new"               # new, waiting, admitted, running, done, rejected, cancelled
+    reason: str = ""
+    columns: int = 0
+    t_submit: float = float("nan")
+    t_admit: float = float("nan")
+    t_launch: float = float("nan")
+    t_done: float = float("nan")
+    result: Optional[list] = None     # per member: dict of device tensors (valid in on_complete)
+    _shapes: list = field(default_factory=list, repr=False)
+    _outputs: object = field(default=None, repr=False)
+    _out_bytes: int = 0
+
+    @property
+    def latency(self):
+        return self.t_done - self.arrival
+
+
+@dataclass
+class _Resident:
+    key: Hashable
+    host: HostMember
+    dev: object = None
+    refs: int = 0
+    last_use: int = 0
+
+
+@dataclass
+class WorkItem:
+    kind: str
+    requests: List[Request]
+    handle: object = None
+    interval: tuple = (float("nan"), float("nan"))   # device (start, end) on the loop's clock
+
+
+class Scheduler:
+    """Admission, residency, batching and completion; the device work goes to ``backend``.
+
+    ``backend`` provides: ``member_bytes(host)``, ``output_bytes(kind, host)``,
+    ``fixed_bytes()``, ``now()``, ``upload(host)`` -> device member, ``release(dev)``,
+    ``alloc_outputs(request, hosts)`` (raises MemoryError when the device refuses),
+    ``free_outputs(request)``, ``launch(kind, requests, devs)`` -> handle,
+    ``done(handle)``, ``completion_time(handle)``, ``device_interval(handle)``,
+    ``retire(handle)``, ``results(request)``, ``start_clock()``, ``synchronize()``.
+    """
+
+    def __init__(self, backend, source: Callable[[Hashable], HostMember], budget_bytes: int,
+                 mode: str = "batched", max_inflight: int = 2, max_batch_columns: int = 1 << 24,
+                 on_complete: Optional[Callable[[Request], None]] = None):
+        if mode not in ("batched", "plain"):
+            raise ValueError("mode is 'batched' or 'plain'")
+        self.b = backend
+        self.source = source
+        self.budget = int(budget_bytes)
+        self.mode = mode
+        self.max_inflight = max_inflight
+        self.max_batch_columns = max_batch_columns
+        self.on_complete = on_complete
+        self.used = self.b.fixed_bytes()
+        if self.used > self.budget:
+            raise ValueError(f"budget {self.budget} below the fixed device bytes {self.used}")
+        self.peak = self.used
+        self.resident: Dict[Hashable, _Resident] = {}
+        self.hosts: Dict[Hashable, HostMember] = {}
+        self.waiting = collections.deque()
+        self.admitted = {TENDENCY: collections.deque(), VJP: collections.deque()}
+        self.inflight: List[WorkItem] = []
+        self.items: List[WorkItem] = []
+        self.finished: List[Request] = []
+        self.cancelled = set()
+        self._rid = 0
+        self._tick = 0
+        self.stats = collections.Counter()
+
+    # -- submission -----------------------------------------------------------------------------
+    def _host(self, key):
+        h = self.hosts.get(key)
+        if h is None:
+            h = self.source(key)
+            self.hosts[key] = h
+        return h
+
+    def submit(self, req: Request) -> Request:
+        req.rid = self._rid
+        self._rid += 1
+        req.t_submit = self.b.now()
+        try:
+            if req.kind not in KINDS:
+                raise ValueError(f"unknown request kind {req.kind!r}")
+            if not req.members:
+                raise ValueError("request names no members")
+            hosts = [self._host(k) for k in req.members]
+        except Exception as e:  # malformed request: unknown member, bad kind, bad data
+            return self._reject(req, f"malformed: {e}")
+        req._shapes = [(h.kx, h.ix, h.il) for h in hosts]
+        req.columns = sum(h.columns for h in hosts)
+        req._out_bytes = sum(self.b.output_bytes(req.kind, h) for h in hosts)
+        distinct = {k: self.hosts[k] for k in req.members}
+        need = req._out_bytes + sum(self.b.member_bytes(h) for h in distinct.values())
+        if self.b.fixed_bytes() + need > self.budget:
+            return self._reject(req, f"needs {need} bytes, budget {self.budget}")
+        req.status = "waiting"
+        self.waiting.append(req)
+        return req
+
+    def _reject(self, req, why):
+        req.status, req.reason = "rejected", why
+        self.stats["rejected"] += 1
+        self.finished.append(req)
+        return req
+
+    def cancel(self, rid) -> bool:
+        for r in list(self.waiting):
+            if r.rid == rid:
+                self.waiting.remove(r)
+                r.status = "cancelled"
+                self.finished.append(r)
+                self.stats["cancelled"] += 1
+                return True
+        for q in self.admitted.values():
+            for r in list(q):
+                if r.rid == rid:
+                    q.remove(r)
+                    self._unpin(r)
+                    self.b.free_outputs(r)
+                    self.used -= r._out_bytes
+                    r.status = "cancelled"
+                    self.finished.append(r)
+                    self.stats["cancelled"] += 1
+                    return True
+        for it in self.inflight:
+            for r in it.requests:
+                if r.rid == rid and r.status == "running":
+                    self.cancelled.add(rid)
+                    return True
+        return False
+
+    # -- residency and admission ----------------------------------------------------------------
+    def _evict_for(self, nbytes, keep):
+        idle = sorted((r for r in self.resident.values() if r.refs == 0 and r.key not in keep),
+                      key=lambda r: r.last_use)
+        for r in idle:
+            if self.budget - self.used >= nbytes:
+                break
+            self.b.release(r.dev)
+            self.used -= self.b.member_bytes(r.host)
+            del self.resident[r.key]
+            self.stats["evictions"] += 1
+        return self.budget - self.used >= nbytes
+
+    def _admit_one(self, req) -> bool:
+        keys = list(dict.fromkeys(req.members))
+        new = [k for k in keys if k not in self.resident]
+        need = req._out_bytes + sum(self.b.member_bytes(self.hosts[k]) for k in new)
+        if not self._evict_for(need, set(keys)):
+            return False
+        try:
+            self.b.alloc_outputs(req, [self.hosts[k] for k in req.members])
+        except MemoryError:
+            self.stats["alloc_failures"] += 1
+            return False
+        self.used += req._out_bytes
+        for k in new:
+            h = self.hosts[k]
+            try:
+                dev = self.b.upload(h)
+            except MemoryError:
+                self.stats["alloc_failures"] += 1
+                self.b.free_outputs(req)
+                self.used -= req._out_bytes
+                return False
+            self.resident[k] = _Resident(k, h, dev)
+            self.used += self.b.member_bytes(h)
+            self.stats["uploads"] += 1
+            self.stats["upload_bytes"] += h.nbytes
+        self._tick += 1
+        for k in req.members:
+            r = self.resident[k]
+            r.refs += 1
+            r.last_use = self._tick
+        self.peak = max(self.peak, self.used)
+        req.status = "admitted"
+        req.t_admit = self.b.now()
+        self.admitted[req.kind].append(req)
+        return True
+
+    def _unpin(self, req):
+        for k in req.members:
+            r = self.resident.get(k)
+            if r is not None:
+                r.refs -= 1
+
+    def admit(self):
+        n = 0
+        while self.waiting and self._admit_one(self.waiting[0]):
+            self.waiting.popleft()
+            n += 1
+        return n
+
+    # -- launching ------------------------------------------------------------------------------
+    def _inflight_of(self, kind):
+        return sum(1 for it in self.inflight if it.kind == kind)
+
+    def _launch(self, kind, reqs):
+        devs = [[self.resident[k].dev for k in r.members] for r in reqs]
+        handle = self.b.launch(kind, reqs, devs)
+        t = self.b.now()
+        for r in reqs:
+            r.status, r.t_launch = "running", t
+        self.inflight.append(WorkItem(kind, reqs, handle))
+        self.stats[f"launches_{kind}"] += 1
+
+    def launch(self):
+        n = 0
+        if self.mode == "plain":
+            if self.inflight:
+                return 0
+            # one request at a time, in admission (= arrival) order across both kinds
+            cands = [q[0] for q in self.admitted.values() if q]
+            if cands:
+                r = min(cands, key=lambda x: x.rid)
+                self.admitted[r.kind].popleft()
+                self._launch(r.kind, [r])
+                n += 1
+            return n
+        q = self.admitted[TENDENCY]
+        while q and self._inflight_of(TENDENCY) < self.max_inflight:
+            batch, cols = [], 0
+            while q and (not batch or cols + q[0].columns <= self.max_batch_columns):
+                r = q.popleft()
+                batch.append(r)
+                cols += r.columns
+            self._launch(TENDENCY, batch)
+            n += 1
+        q = self.admitted[VJP]
+        while q and self._inflight_of(VJP) < self.max_inflight:
+            self._launch(VJP, [q.popleft()])
+            n += 1
+        return n
+
+    # -- completion -----------------------------------------------------------------------------
+    def poll(self):
+        n = 0
+        for it in list(self.inflight):
+            if not self.b.done(it.handle):
+                continue
+            t = self.b.completion_time(it.handle)
+            it.interval = self.b.device_interval(it.handle)
+            self.inflight.remove(it)
+            self.items.append(it)
+            for r in it.requests:
+                r.t_done = t
+                if r.rid in self.cancelled:
+                    r.status = "cancelled"
+                    self.stats["cancelled"] += 1
+                else:
+                    r.status = "done"
+                    if self.on_complete is not None:
+                        r.result = self.b.results(r)
+                        self.on_complete(r)
+                        r.result = None
+                self._unpin(r)
+                self.b.free_outputs(r)
+                self.used -= r._out_bytes
+                self.finished.append(r)
+                n += 1
+            self.b.retire(it.handle)
+        return n
+
+    def busy(self):
+        return bool(self.waiting or self.inflight or any(self.admitted.values()))
+
+    def step(self):
+        """One pass of the loop: retire, admit, launch.  Returns the amount of work done."""
+        return self.poll() + self.admit() + self.launch()
+
+    def run(self, requests: List[Request], timeout_s: float = 600.0):
+        """Serve ``requests`` (their ``arrival`` times in seconds after the start) in real time
+        and return the finished requests."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        self.b.start_clock()
+        t_end = time.perf_counter() + timeout_s
+        while pending or self.busy():
+            now = self.b.now()
+            while pending and pending[0].arrival <= now:
+                self.submit(pending.popleft())
+            if self.step() == 0 and time.perf_counter() > t_end:
+                raise TimeoutError(f"serving loop exceeded {timeout_s} s "
+                                   f"({len(pending)} pending, {len(self.inflight)} in flight)")
+        self.b.synchronize()
+        return self.finished
+
+
+def latency_stats(finished: List[Request]):
+    """p50/p99 latency (ms) overall and per kind, and columns/s over the run."""
+    done = [r for r in finished if r.status == "done"]
+    if not done:
+        return dict(requests=0)
+    lat = np.array([r.latency for r in done]) * 1e3
+    t0 = min(r.arrival for r in done)
+    t1 = max(r.t_done for r in done)
+    out = dict(requests=len(done), p50_ms=float(np.percentile(lat, 50)),
+               p99_ms=float(np.percentile(lat, 99)), mean_ms=float(lat.mean()),
+               max_ms=float(lat.max()), columns=int(sum(r.columns for r in done)),
+               makespan_s=float(t1 - t0))
+    out["columns_per_s"] = out["columns"] / max(t1 - t0, 1e-9)
+    for kind in KINDS:
+        sel = np.array([r.latency for r in done if r.kind == kind]) * 1e3
+        if sel.size:
+            out[f"{kind}_p50_ms"] = float(np.percentile(sel, 50))
+            out[f"{kind}_p99_ms"] = float(np.percentile(sel, 99))
+            out[f"{kind}_requests"] = int(sel.size)
+            out[f"{kind}_columns"] = int(sum(r.columns for r in done if r.kind == kind))
+    return out
+
+
+def overlap_stats(items: List[WorkItem]):
+    """Device time of the tendency and VJP work items, and how much of the VJP time ran
+    while a tendency batch was also on the device."""
+    iv = {k: sorted(it.interval for it in items if it.kind == k) for k in KINDS}
+    busy = {k: float(sum(b - a for a, b in v)) for k, v in iv.items()}
+    both = 0.0
+    for a, b in iv[VJP]:
+        for c, d in iv[TENDENCY]:
+            if c >= b:
+                break
+            both += max(0.0, min(b, d) - max(a, c))
+    return dict(tendency_busy_s=busy[TENDENCY], vjp_busy_s=busy[VJP], overlap_s=both,
+                vjp_overlap_fraction=both / busy[VJP] if busy[VJP] > 0 else 0.0)
+
+
+# Resolutions and level counts of the request stream (spectral truncation -> (ix, il)).
+STREAM_GRIDS = {21: (64, 32), 31: (96, 48), 42: (128, 64), 85: (256, 128), 170: (512, 256)}
+
+
+def poisson_stream(seed=0, rate=200.0, n=400, vjp_fraction=0.2, max_members=32,
+                   truncations=(21, 31, 42, 85, 170), levels=(8, 16), member_pool=8):
+    """Requests of the serving workload: Poisson arrivals at ``rate`` per second, tendency or
+    VJP (``vjp_fraction``), 1..``max_members`` members at one resolution and level count drawn
+    uniformly.  Member keys are (truncation, kx, seed) with seeds from a pool of
+    ``member_pool`` per (truncation, kx), so member state is shared across requests."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n)) if rate > 0 else np.zeros(n)
+    reqs = []
+    for i in range(n):
+        trunc = int(rng.choice(truncations))
+        kx = int(rng.choice(levels))
+        m = int(rng.integers(1, max_members + 1))
+        s0 = int(rng.integers(0, member_pool))
+        kind = VJP if rng.uniform() < vjp_fraction else TENDENCY
+        keys = [(trunc, kx, (s0 + j) % member_pool) for j in range(m)]
+        reqs.append(Request(kind, keys, arrival=float(t[i]), seed=int(rng.integers(1 << 30))))
+    return reqs
+
+
+def synthetic_member(key, base_seed=5000):
+    """The synthetic land member (an Instance) that a ``poisson_stream`` key names."""
+    from . import synthetic
+    trunc, kx, s = key
+    ix, il = STREAM_GRIDS[trunc]
+    return synthetic.land_instance(base_seed + 1000 * trunc + 100 * kx + s, ix, il, kx)
+
+
+def synthetic_source(base_seed=5000, pin=True):
+    """Member source for ``poisson_stream`` keys: land members of the synthetic generator."""
+    cache = {}
+
+    def source(key):
+        if key not in cache:
+            cache[key] = HostMember.from_instance(synthetic_member(key, base_seed), pin=pin)
+        return cache[key]
+    return source
+
+
+# ---------------------------------------------------------------------------------------------
+# CUDA backend
+# ---------------------------------------------------------------------------------------------
+class _DevMember:
+    __slots__ = ("host", "buf", "inputs", "ready")
+
+    def __init__(self, host, buf, inputs, ready):
+        self.host, self.buf, self.inputs, self.ready = host, buf, inputs, ready
+
+
+class _Handle:
+    __slots__ = ("stream", "start", "done", "keep")
+
+    def __init__(self, stream, start, done, keep):
+        self.stream, self.start, self.done, self.keep = stream, start, done, keep
+
+
+class CudaBackend:
+    """Device work of the serving loop through the C ABI (ensemble, plain and VJP calls)."""
+
+    def __init__(self, device="cuda", date=None, parameters=None, mode="batched"):
+        import torch
+        from .physics import DateData, SpeedyPhysics, initialize_vertical
+        self.torch = torch
+        self.lib = _lib.load()
+        self.dev = torch.device(device)
+        if self.dev.index is None:
+            self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.mode = mode
+        self.date = date or DateData(80.0 / 365.2425, 1950, 0, 1800.0)
+        self.phys = SpeedyPhysics(parameters, diagnostics=False)
+        self.compute = torch.cuda.Stream(self.dev)
+        self.vjp_stream = torch.cuda.Stream(self.dev) if mode == "batched" else self.compute
+        self.copy = torch.cuda.Stream(self.dev) if mode == "batched" else self.compute
+        self._vg = {}
+        self._vert = initialize_vertical
+        # adjoint scratch: one buffer, reused in stream order on the VJP stream
+        self._vjp_bytes = max(self._vjp_scratch_bytes(kx) for kx in (8, 16))
+        self._fwd_bytes = self._fwd_scratch_bytes()
+        with torch.cuda.stream(self.vjp_stream):
+            self.vjp_scratch = torch.empty(self._vjp_bytes, dtype=torch.uint8, device=self.dev)
+        with torch.cuda.stream(self.compute):
+            self.fwd_scratch = torch.empty(self._fwd_bytes, dtype=torch.uint8, device=self.dev)
+        self._t0 = None
+        self._h0 = 0.0
+
+    # -- sizes ----------------------------------------------------------------------------------
+    def _desc(self, kx, ix, il, lfluxland):
+        from types import SimpleNamespace
+        return self.phys.desc(SimpleNamespace(nodal_shape=(kx, ix, il)), self.date, lfluxland)
+
+    def _vjp_scratch_bytes(self, kx):
+        # 512 x 256 columns reach the adjoint's thread cap, hence its largest scratch
+        d = self._desc(kx, 512, 256, True)
+        return int(self.lib.spd_vjp_scratch_bytes(C.byref(d)))
+
+    def _fwd_scratch_bytes(self):
+        d = self._desc(16, 512, 256, True)
+        return int(self.lib.spd_fwd_scratch_bytes(C.byref(d)))
+
+    def vgrid(self, kx):
+        if kx not in self._vg:
+            from .physics import Geometry
+            g = Geometry.__new__(Geometry)
+            vert = self._vert(kx)
+            for n, v in zip(("hsg", "fsg", "dhs", "sigl", "grdsig", "grdscp", "wvi"), vert):
+                setattr(g, n, v)
+            g.nodal_shape = (kx, 1, 1)
+            g._vgrid = None
+            self._vg[kx] = g.vgrid()
+        return self._vg[kx]
+
+    def fixed_bytes(self):
+        return self._vjp_bytes + self._fwd_bytes
+
+    def member_bytes(self, h):
+        return h.nbytes
+
+    def output_bytes(self, kind, h):
+        f = tendency_result_floats if kind == TENDENCY else vjp_result_floats
+        return _round_up(4 * f(h.kx, h.ix, h.il))
+
+    # -- clock ----------------------------------------------------------------------------------
+    def start_clock(self):
+        torch = self.torch
+        torch.cuda.synchronize(self.dev)
+        self._t0 = torch.cuda.Event(enable_timing=True)
+        self._t0.record(self.compute)
+        self._t0.synchronize()
+        self._h0 = time.perf_counter()
+
+    def now(self):
+        return time.perf_counter() - self._h0
+
+    def synchronize(self):
+        self.torch.cuda.synchronize(self.dev)
+
+    # -- memory ---------------------------------------------------------------------------------
+    def upload(self, h):
+        torch = self.torch
+        try:
+            with torch.cuda.stream(self.copy):
+                buf = torch.empty(h.nbytes, dtype=torch.uint8, device=self.dev)
+                buf.copy_(h.buffer, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.copy)
+        except torch.cuda.OutOfMemoryError as e:
+            raise MemoryError(str(e))
+        base = buf.data_ptr()
+        off, _ = member_layout(h.kx, h.ix, h.il)
+        inputs = _lib.Inputs(**{n: base + off[n][0] for n in _lib.INPUT_FIELDS})
+        return _DevMember(h, buf, inputs, ev)
+
+    def release(self, dm):
+        dm.buf = None
+
+    def alloc_outputs(self, req, hosts):
+        torch = self.torch
+        stream = self.compute if req.kind == TENDENCY else self.vjp_stream
+        f = tendency_result_floats if req.kind == TENDENCY else vjp_result_floats
+        sizes = [_round_up(4 * f(h.kx, h.ix, h.il)) // 4 for h in hosts]
+        try:
+            with torch.cuda.stream(stream):
+                req._outputs = torch.empty(sum(sizes), dtype=torch.float32, device=self.dev)
+        except torch.cuda.OutOfMemoryError as e:
+            raise MemoryError(str(e))
+        views, pos = [], 0
+        for h, n in zip(hosts, sizes):
+            c, kx = h.ix * h.il, h.kx
+            o = req._outputs[pos:pos + n]
+            d, p = {}, 0
+            shape3, shape2 = (kx, h.ix, h.il), (h.ix, h.il)
+            if req.kind == TENDENCY:
+                names = [(k, shape3) for k in ("u_wind", "v_wind", "temperature",
+                                               "specific_humidity")]
+                names += [("precnv", shape2), ("precls", shape2)]
+            else:
+                names = [(k, shape3) for k in ("u_wind", "v_wind", "temperature",
+                                               "specific_humidity", "geopotential")]
+                names += [("normalized_surface_pressure", shape2), ("params", (12,))]
+                names += [("ct_" + k, shape3) for k in ("u_wind", "v_wind", "temperature",
+                                                        "specific_humidity")]
+            for k, shp in names:
+                m = int(np.prod(shp))
+                d[k] = o[p:p + m].view(shp)
+                p += m
+            views.append(d)
+            pos += n
+        req._views = views
+
+    def free_outputs(self, req):
+        req._outputs = None
+        req._views = None
+
+    def results(self, req):
+        return req._views
+
+    # -- launches -------------------------------------------------------------------------------
+    def launch(self, kind, reqs, devs):
+        torch = self.torch
+        if kind == VJP:
+            stream = self.vjp_stream
+        else:
+            stream = self.compute
+        start = torch.cuda.Event(enable_timing=True)
+        done = torch.cuda.Event(enable_timing=True)
+        keep = []
+        with torch.cuda.stream(stream):
+            seen = set()
+            for dl in devs:
+                for dm in dl:
+                    if id(dm) not in seen:
+                        seen.add(id(dm))
+                        stream.wait_event(dm.ready)
+                        dm.buf.record_stream(stream)
+            start.record(stream)
+            if kind == VJP:
+                for r, dl in zip(reqs, devs):
+                    self._vjp(r, dl, stream)
+            elif self.mode == "plain":
+                for r, dl in zip(reqs, devs):
+                    for dm, out in zip(dl, r._views):
+                        self._fwd_plain(dm, out, stream)
+            else:
+                keep.append(self._ensemble(reqs, devs, stream))
+            done.record(stream)
+        return _Handle(stream, start, done, keep)
+
+    def _outputs_struct(self, out):
+        return _lib.Outputs(**{k: (out[k].data_ptr() if k in out else None)
+                               for k in _lib.OUTPUT_FIELDS})
+
+    def _fwd_plain(self, dm, out, stream):
+        h = dm.host
+        desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+        rc = self.lib.spd_fwd(C.byref(desc), C.byref(self.vgrid(h.kx)),
+                              C.byref(self.phys._pstruct), C.byref(dm.inputs),
+                              C.byref(self._outputs_struct(out)),
+                              C.c_void_p(self.fwd_scratch.data_ptr()), self._fwd_bytes,
+                              C.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "spd_fwd")
+
+    def _vjp(self, req, dl, stream):
+        torch = self.torch
+        for i, (dm, out) in enumerate(zip(dl, req._views)):
+            g = torch.Generator(device=self.dev)
+            g.manual_seed(int(req.seed) * 1009 + i)
+            for k in ("u_wind", "v_wind", "temperature", "specific_humidity"):
+                out["ct_" + k].normal_(generator=g)
+            h = dm.host
+            desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+            cts = _lib.Cotangents(**{k: out["ct_" + k].data_ptr()
+                                     for k in ("u_wind", "v_wind", "temperature",
+                                               "specific_humidity")})
+            grads = _lib.Grads(**{k: out[k].data_ptr() for k in
+                                  ("u_wind", "v_wind", "temperature", "specific_humidity",
+                                   "geopotential", "normalized_surface_pressure", "params")})
+            rc = self.lib.spd_vjp(C.byref(desc), C.byref(self.vgrid(h.kx)),
+                                  C.byref(self.phys._pstruct), C.byref(dm.inputs), C.byref(cts),
+                                  C.byref(grads), C.c_void_p(self.vjp_scratch.data_ptr()),
+                                  self._vjp_bytes, C.c_void_p(stream.cuda_stream))
+            _lib.check(rc, "spd_vjp")
+
+    def _ensemble(self, reqs, devs, stream):
+        torch = self.torch
+        classes, cls_of = [], {}
+        members = []
+        for r, dl in zip(reqs, devs):
+            for dm, out in zip(dl, r._views):
+                h = dm.host
+                key = (h.kx, h.lfluxland)
+                if key not in cls_of:
+                    c = _lib.Class()
+                    c.desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+                    c.vgrid = self.vgrid(h.kx)
+                    c.params = self.phys._pstruct
+                    cls_of[key] = len(classes)
+                    classes.append(c)
+                members.append((dm, out, cls_of[key]))
+        if len(classes) > _lib.MAX_CLASSES:
+            raise ValueError("more member classes than one ensemble launch takes")
+        mem = (_lib.Member * len(members))()
+        for i, (dm, out, ci) in enumerate(members):
+            mem[i].inp = dm.inputs
+            mem[i].out = self._outputs_struct(out)
+            mem[i].ix, mem[i].il, mem[i].cls = dm.host.ix, dm.host.il, ci
+        cl = (_lib.Class * len(classes))(*classes)
+        nbytes = int(self.lib.spd_ensemble_plan_bytes(mem, len(members)))
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        plan = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        info = _lib.PlanInfo()
+        rc = self.lib.spd_ensemble_plan(cl, len(classes), mem, len(members),
+                                        C.c_void_p(host.data_ptr()),
+                                        C.c_void_p(plan.data_ptr()), nbytes, C.byref(info))
+        _lib.check(rc, "spd_ensemble_plan")
+        plan.copy_(host, non_blocking=True)
+        rc = self.lib.spd_ensemble_fwd(cl, len(classes), C.c_void_p(plan.data_ptr()),
+                                       C.byref(info), 0, C.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "spd_ensemble_fwd")
+        return (host, plan, cl, mem)
+
+    def done(self, handle):
+        return handle.done.query()
+
+    def completion_time(self, handle):
+        """Device completion of the work item, in seconds on the loop's clock (``now``)."""
+        return self._t0.elapsed_time(handle.done) / 1e3
+
+    def device_interval(self, handle):
+        """(start, end) of the work item in seconds on the loop's clock."""
+        return (self._t0.elapsed_time(handle.start) / 1e3,
+                self._t0.elapsed_time(handle.done) / 1e3)
+
+    def retire(self, handle):
+        handle.keep = None

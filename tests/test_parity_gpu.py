@@ -13,9 +13,7 @@ import importlib
 import numpy as np
 import pytest
 
-from oracle import speedy_oracle as O
-from tests.helpers import (compare_fields, oracle_f64, parity_summary, run_gpu_instance,
-                           x64_errors, x64_violations)
+from tests.helpers import parity_check
 
 pytestmark = pytest.mark.gpu
 
@@ -26,22 +24,7 @@ def pkg():
 
 
 def check(pkg, inst, params=None, max_flip_frac=2e-3, **kw):
-    got = run_gpu_instance(pkg, inst, params=params, **kw)
-    args = list(inst.oracle_args(O.default_parameters()))
-    rec = O.Margins((inst.ix, inst.il))
-    step = O.physics_step if kw.get("fuse_verify") else O.compute_tendencies
-    tend, data = step(*args, rec=rec)
-    ref64 = step(*oracle_f64(inst))
-    rep = compare_fields(got, tend, data, ref64)
-    summ = parity_summary(rep, (inst.ix, inst.il), rec.ulps)
-    cols = summ.pop("_cols")
-    x64 = x64_errors(got, tend, data, ref64, exclude_cols=cols)
-    print(inst.name, {k: (v["nbad"], f"{v['norm']:.1e}") for k, v in rep.items()}, summ,
-          {k: (f"{a:.1e}", f"{b:.1e}") for k, (a, b) in x64.items()})
-    assert summ["unexplained_columns"] == 0, (summ, {k: v["nbad"] for k, v in rep.items()})
-    assert summ["flip_columns"] <= max(2, max_flip_frac * summ["columns"]), summ
-    assert not x64_violations(x64), x64_violations(x64)
-    return rep, summ
+    return parity_check(pkg, inst, params=params, max_flip_frac=max_flip_frac, **kw)
 
 
 @pytest.mark.parametrize("lfluxland", [False, True])

@@ -1,0 +1,302 @@
+"""Serving loop logic on the CPU: admission by budget, residency and eviction, continuous
+batching, plain (one request at a time) order, rejection of malformed and oversized requests,
+allocation failures, cancellation, and the request stream generator.  The device is a fake
+backend on a virtual clock: a launched work item takes (columns x cost) seconds on its stream."""
+import importlib
+
+import numpy as np
+import pytest
+
+pkg = importlib.import_module("jax-gcm_b200")
+S = pkg.serving
+
+
+class FakeBackend:
+    def __init__(self, fixed=0, per_col=1e-6, fail_alloc=0, realtime=False):
+        self.t = 0.0
+        self.fixed = fixed
+        self.per_col = per_col
+        self.fail_alloc = fail_alloc
+        self.realtime = realtime
+        self.uploaded, self.released, self.launched = [], [], []
+        self.stream_free = {S.TENDENCY: 0.0, S.VJP: 0.0}
+        self._h0 = 0.0
+
+    def fixed_bytes(self):
+        return self.fixed
+
+    def member_bytes(self, h):
+        return h.nbytes
+
+    def output_bytes(self, kind, h):
+        return 4 * h.columns * (4 * h.kx + 2 if kind == S.TENDENCY else 9 * h.kx + 1)
+
+    def now(self):
+        if self.realtime:
+            import time
+            return time.perf_counter() - self._h0
+        return self.t
+
+    def start_clock(self):
+        import time
+        self._h0 = time.perf_counter()
+
+    def synchronize(self):
+        pass
+
+    def upload(self, h):
+        self.uploaded.append(h)
+        return ("dev", id(h))
+
+    def release(self, d):
+        self.released.append(d)
+
+    def alloc_outputs(self, req, hosts):
+        if self.fail_alloc > 0:
+            self.fail_alloc -= 1
+            raise MemoryError("injected allocation failure")
+        req._outputs = [dict(n=h.columns) for h in hosts]
+
+    def free_outputs(self, req):
+        req._outputs = None
+
+    def results(self, req):
+        return req._outputs
+
+    def launch(self, kind, reqs, devs):
+        cols = sum(r.columns for r in reqs)
+        start = max(self.now(), self.stream_free[kind])
+        end = start + cols * self.per_col
+        self.stream_free[kind] = end
+        self.launched.append((kind, [r.rid for r in reqs]))
+        return dict(start=start, end=end)
+
+    def done(self, h):
+        return self.now() >= h["end"]
+
+    def completion_time(self, h):
+        return h["end"]
+
+    def device_interval(self, h):
+        return (h["start"], h["end"])
+
+    def retire(self, h):
+        pass
+
+
+def host(kx=8, ix=64, il=32, nbytes=None):
+    n = nbytes if nbytes is not None else S.member_layout(kx, ix, il)[1]
+    return S.HostMember(kx, ix, il, True, None, n)
+
+
+def make_source(**shapes):
+    hosts = {k: host(*v) if isinstance(v, tuple) else v for k, v in shapes.items()}
+
+    def source(key):
+        return hosts[key]
+    return source, hosts
+
+
+def test_member_layout_is_aligned_and_complete():
+    off, n = S.member_layout(16, 96, 48)
+    assert [k for k in off] == list(pkg._lib.INPUT_FIELDS)
+    for name, (pos, cnt) in off.items():
+        assert pos % 256 == 0
+        exp = 16 * 96 * 48 if name in ("u_wind", "v_wind", "temperature", "specific_humidity",
+                                       "geopotential") else (48 if name in ("sia", "coa")
+                                                             else 96 * 48)
+        assert cnt == exp, name
+    assert n >= 4 * (5 * 16 * 96 * 48 + 10 * 96 * 48 + 2 * 48)
+
+
+def test_host_member_packs_instance_fields():
+    inst = pkg.synthetic.land_instance(3, 8, 4, 8)
+    h = S.HostMember.from_instance(inst, pin=False)
+    off, n = S.member_layout(8, 8, 4)
+    flat = h.buffer.view(-1).numpy().view(np.float32)
+    pos, cnt = off["temperature"]
+    assert np.array_equal(flat[pos // 4: pos // 4 + cnt], inst.t.ravel())
+    pos, cnt = off["coa"]
+    assert np.array_equal(flat[pos // 4: pos // 4 + cnt], inst.coa)
+    assert h.nbytes == n and h.columns == 32
+
+
+def test_continuous_batching_merges_arrivals_while_busy():
+    src, _ = make_source(a=(8, 64, 32), b=(16, 64, 32), c=(8, 96, 48))
+    be = FakeBackend(per_col=1e-6)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30, max_inflight=2)
+    for k in ("a", "b", "c"):
+        sch.submit(S.Request(S.TENDENCY, [k]))
+    sch.step()
+    assert be.launched == [(S.TENDENCY, [0, 1, 2])]          # one batch of three
+    sch.submit(S.Request(S.TENDENCY, ["a", "b"]))
+    sch.submit(S.Request(S.TENDENCY, ["c"]))
+    sch.step()
+    assert be.launched[-1] == (S.TENDENCY, [3, 4])            # second batch while first runs
+    sch.submit(S.Request(S.TENDENCY, ["a"]))
+    sch.step()
+    assert len(be.launched) == 2                              # two in flight: waits
+    assert [r.rid for r in sch.admitted[S.TENDENCY]] == [5]
+    be.t = 1.0
+    sch.step()
+    assert be.launched[-1] == (S.TENDENCY, [5])
+    be.t = 2.0
+    sch.step()
+    assert not sch.busy()
+    assert [r.status for r in sch.finished] == ["done"] * 6
+    assert len(be.uploaded) == 3                              # members stay resident
+
+
+def test_vjp_requests_run_on_their_own_stream_and_overlap():
+    src, _ = make_source(a=(8, 128, 64), b=(16, 128, 64))
+    be = FakeBackend(per_col=1e-6)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30)
+    sch.submit(S.Request(S.TENDENCY, ["a"]))
+    sch.submit(S.Request(S.VJP, ["b"]))
+    sch.step()
+    kinds = sorted(k for k, _ in be.launched)
+    assert kinds == [S.TENDENCY, S.VJP]
+    be.t = 10.0
+    sch.step()
+    ov = S.overlap_stats(sch.items)
+    assert ov["overlap_s"] > 0 and 0 < ov["vjp_overlap_fraction"] <= 1
+
+
+def test_plain_mode_is_one_request_at_a_time_in_arrival_order():
+    src, _ = make_source(a=(8, 64, 32), b=(16, 64, 32))
+    be = FakeBackend(per_col=1e-6)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30, mode="plain")
+    sch.submit(S.Request(S.VJP, ["a"]))
+    sch.submit(S.Request(S.TENDENCY, ["b"]))
+    sch.submit(S.Request(S.TENDENCY, ["a"]))
+    for step in range(10):
+        be.t = float(step)
+        sch.step()
+        assert len(sch.inflight) <= 1
+    order = [ids for _, ids in be.launched]
+    assert order == [[0], [1], [2]]
+
+
+def test_budget_admission_eviction_and_fifo():
+    out = 4 * (4 * 8 + 2) * 64 * 32       # one member's tendency outputs
+    m = 10 * out                          # one member's resident state
+    hosts = dict(a=host(8, 64, 32, nbytes=m), b=host(8, 64, 32, nbytes=m),
+                 c=host(8, 64, 32, nbytes=m))
+    src = hosts.__getitem__
+    budget = 2 * m + 2 * out + 10         # r0's members and outputs; no room for r1 beside
+    be = FakeBackend(per_col=1e-3)
+    sch = S.Scheduler(be, src, budget_bytes=budget)
+    r0 = sch.submit(S.Request(S.TENDENCY, ["a", "b"]))
+    r1 = sch.submit(S.Request(S.TENDENCY, ["c"]))
+    sch.step()
+    assert r0.status == "running" and r1.status == "waiting"
+    assert sch.used <= budget
+    be.t = 100.0
+    sch.step()                            # r0 done; r1 admitted after evicting an idle member
+    assert r0.status == "done" and r1.status in ("running", "done")
+    assert sch.stats["evictions"] >= 1
+    assert sch.peak <= budget
+    be.t = 200.0
+    sch.step()
+    assert r1.status == "done" and sch.used == be.fixed_bytes() + sum(
+        h.nbytes for k, h in hosts.items() if k in sch.resident)
+
+
+def test_resident_members_in_use_are_never_evicted():
+    hosts = dict(a=host(nbytes=1000), b=host(nbytes=1000))
+    out = 4 * (4 * 8 + 2) * 64 * 32
+    be = FakeBackend(per_col=1e-3)
+    sch = S.Scheduler(be, hosts.__getitem__, budget_bytes=1000 + out + 500)
+    r0 = sch.submit(S.Request(S.TENDENCY, ["a"]))
+    r1 = sch.submit(S.Request(S.TENDENCY, ["b"]))
+    sch.step()
+    assert r0.status == "running" and r1.status == "waiting"
+    assert "a" in sch.resident and sch.resident["a"].refs == 1
+    assert not be.released
+
+
+def test_rejections_malformed_and_oversized():
+    hosts = dict(a=host(nbytes=1000))
+    be = FakeBackend()
+    sch = S.Scheduler(be, hosts.__getitem__, budget_bytes=10_000)
+    r = sch.submit(S.Request(S.TENDENCY, ["missing"]))
+    assert r.status == "rejected" and r.reason.startswith("malformed")
+    r = sch.submit(S.Request("forecast", ["a"]))
+    assert r.status == "rejected" and "kind" in r.reason
+    r = sch.submit(S.Request(S.TENDENCY, []))
+    assert r.status == "rejected"
+    r = sch.submit(S.Request(S.TENDENCY, ["a"]))      # outputs alone exceed the budget
+    assert r.status == "rejected" and "budget" in r.reason
+    assert sch.stats["rejected"] == 4 and not sch.busy()
+
+
+def test_allocation_failure_is_retried():
+    src, _ = make_source(a=(8, 64, 32))
+    be = FakeBackend(fail_alloc=2)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30)
+    r = sch.submit(S.Request(S.TENDENCY, ["a"]))
+    sch.step()
+    assert r.status == "waiting"
+    sch.step()
+    assert r.status == "waiting"
+    sch.step()
+    assert r.status == "running"
+    assert sch.stats["alloc_failures"] == 2
+
+
+def test_cancel_waiting_and_inflight():
+    src, hosts = make_source(a=(8, 64, 32), b=(8, 64, 32))
+    seen = []
+    be = FakeBackend(per_col=1e-3)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30, mode="plain", on_complete=seen.append)
+    r0 = sch.submit(S.Request(S.TENDENCY, ["a"]))
+    r1 = sch.submit(S.Request(S.TENDENCY, ["b"]))
+    sch.step()
+    assert r0.status == "running"
+    assert sch.cancel(r1.rid) and r1.status == "cancelled"
+    assert sch.cancel(r0.rid)
+    be.t = 100.0
+    sch.step()
+    assert r0.status == "cancelled" and not seen
+    assert not sch.busy() and sch.used == sum(
+        h.nbytes for k, h in hosts.items() if k in sch.resident)
+    assert not sch.cancel(12345)
+
+
+def test_run_loop_real_time_with_fake_device():
+    src, _ = make_source(a=(8, 64, 32), b=(16, 96, 48))
+    be = FakeBackend(per_col=1e-8, realtime=True)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30)
+    reqs = [S.Request(S.TENDENCY if i % 3 else S.VJP, ["a", "b"][: 1 + i % 2],
+                      arrival=0.002 * i) for i in range(20)]
+    fin = sch.run(reqs, timeout_s=30)
+    st = S.latency_stats(fin)
+    assert st["requests"] == 20 and st["p99_ms"] >= st["p50_ms"] >= 0
+    assert all(r.t_done >= r.arrival for r in fin)
+
+
+def test_poisson_stream_shape():
+    reqs = S.poisson_stream(seed=4, rate=200.0, n=2000)
+    t = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(t) >= 0)
+    assert abs(np.mean(np.diff(t)) - 1 / 200) < 0.0005
+    frac = np.mean([r.kind == S.VJP for r in reqs])
+    assert 0.17 < frac < 0.23
+    sizes = [len(r.members) for r in reqs]
+    assert min(sizes) == 1 and max(sizes) == 32
+    assert {k[0] for r in reqs for k in r.members} == {21, 31, 42, 85, 170}
+    assert {k[1] for r in reqs for k in r.members} == {8, 16}
+    assert S.poisson_stream(seed=4, n=5)[3].members == S.poisson_stream(seed=4, n=5)[3].members
+
+
+def test_latency_stats():
+    rs = []
+    for i in range(100):
+        r = S.Request(S.TENDENCY, ["a"], arrival=i * 0.01)
+        r.status, r.t_done, r.columns = "done", i * 0.01 + 0.001 * (i + 1), 10
+        rs.append(r)
+    st = S.latency_stats(rs)
+    assert st["requests"] == 100
+    assert st["p50_ms"] == pytest.approx(50.5, rel=1e-6)
+    assert st["p99_ms"] == pytest.approx(99.01, rel=1e-6)
+    assert st["columns"] == 1000
