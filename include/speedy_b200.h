@@ -134,12 +134,14 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 /* Adjoint (vector-Jacobian product) of the plain forward.                                    */
 /* Replaces jax.vjp of SpeedyPhysics.compute_tendencies (speedy_physics.py:88-127; the         */
 /* reference differentiates through jax.checkpoint-ed terms, speedy_physics.py:82-86).         */
-/* Each thread re-evaluates its column's forward recording a reverse-mode tape in `scratch`    */
-/* (recompute in column, nothing stored from the forward call) and sweeps it backwards.        */
-/* Ties of min/max split the derivative 0.5/0.5 (JAX's lax.min/lax.max rule); integer levels  */
-/* and the instance level set carry no derivative.                                            */
+/* One thread per column re-evaluates the column's forward (nothing is kept from the forward  */
+/* call) and runs a hand-written reverse pass over its terms.  Ties of min/max split the      */
+/* derivative 0.5/0.5 (JAX's lax.min/lax.max rule); integer levels and the instance level set */
+/* carry no derivative.  With SPD_FUSE_VERIFY set the VJP is that of the fused step           */
+/* (verify_state, the physics, verify_tendencies and the humidity scale), and the humidity   */
+/* gradient is with respect to the humidity as given.  `scratch` holds the level-set word and  */
+/* the per-latitude solar table: spd_vjp_scratch_bytes(desc) bytes, 256-byte aligned.          */
 /* ----------------------------------------------------------------------------------------- */
-#define SPD_VJP_MAX_THREADS 32768
 #define SPD_NUM_DIFF_PARAMS 12
 
 /* Cotangents of the four tendency planes [kx][C]. */

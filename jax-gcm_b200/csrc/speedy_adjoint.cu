@@ -1,18 +1,17 @@
-// speedy_adjoint.cu -- recompute-in-column adjoint of the plain forward (spd_vjp).
+// speedy_adjoint.cu -- the adjoint of the plain forward (spd_vjp).
 //
 // Launch 1 is the forward's cloud-top pre-pass (the instance level set S and the per-latitude
-// solar table: neither carries a derivative).  Launch 2 gives every thread a slice of the tape
-// scratch; per column it records the column's forward on the tape (speedy_generic.h with
-// R = Adj<float>), seeds the output adjoints with the cotangents, sweeps the tape once and
-// writes the input gradients.  The 12 parameter gradients are summed per thread, then per block,
-// then with one atomicAdd per block and parameter.
+// solar table: neither carries a derivative).  Launch 2 runs one thread per column: the
+// hand-written reverse pass of speedy_vjp.h recomputes the column's forward and walks its terms
+// backwards, writing the state gradients.  The 12 parameter gradients are summed per thread,
+// then per block, then with one atomicAdd per block and parameter.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <algorithm>
 
-#include "speedy_generic.h"
 #include "speedy_kernels.cuh"
+#include "speedy_vjp.h"
 
 namespace spd {
 
@@ -20,133 +19,82 @@ int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_output
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
 constexpr size_t kAdjHeader = 256;
-
-inline int tape_cap(int kx) { return 320 * kx + 512; }
-
-inline int vjp_threads(int C) {
-  const int t = ((C + kBlock - 1) / kBlock) * kBlock;
-  return std::min(t, SPD_VJP_MAX_THREADS);
-}
+constexpr int kAdjBlock = 128;
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-struct VjpLayout {
-  size_t table, ia, ib, pa, pb, adj, total;
-  int cap, nthreads;
-};
-
-inline VjpLayout vjp_layout(const spd_desc_t* d) {
-  VjpLayout L;
-  const int C = d->ix * d->il;
-  L.cap = tape_cap(d->kx);
-  L.nthreads = vjp_threads(C);
-  const size_t per = (size_t)L.cap * L.nthreads * 4;
-  L.table = kAdjHeader;
-  L.ia = L.table + align256((size_t)d->il * sizeof(ZonalRow));
-  L.ib = L.ia + align256(per);
-  L.pa = L.ib + align256(per);
-  L.pb = L.pa + align256(per);
-  L.adj = L.pb + align256(per);
-  L.total = L.adj + align256(per);
-  return L;
+inline size_t vjp_scratch(const spd_desc_t* d) {
+  return kAdjHeader + align256((size_t)d->il * sizeof(ZonalRow));
 }
 
 struct VjpArgs {
   spd_vgrid_t vg;
   spd_params_t p;
   uint32_t flags;
-  int model_step, C, il, cap;
+  int model_step, C, il;
   float ablco2, dt_seconds, q_tend_scale;
 };
 
 template <int KX>
-__global__ void __launch_bounds__(kBlock) adjoint_kernel(const VjpArgs A, const spd_inputs_t in,
-                                                         const spd_cotangents_t ct,
-                                                         const spd_grads_t gr,
-                                                         const uint32_t* __restrict__ S,
-                                                         const ZonalRow* __restrict__ table,
-                                                         int32_t* ia, int32_t* ib, float* pa,
-                                                         float* pb, float* adj,
-                                                         uint32_t* status) {
-  using spdad::Adj;
-  typedef Adj<float> AF;
-  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nthr = gridDim.x * blockDim.x;
-  spdad::TapeT<float> tp{ia + gtid, ib + gtid, pa + gtid, pb + gtid, adj + gtid,
-                         (size_t)nthr, 0, A.cap, 0};
+__global__ void __launch_bounds__(kAdjBlock)
+    adjoint_kernel(const __grid_constant__ VjpArgs A, const spd_inputs_t in,
+                   const spd_cotangents_t ct, const spd_grads_t gr,
+                   const uint32_t* __restrict__ S, const ZonalRow* __restrict__ table) {
   const int C = A.C;
-  const uint32_t Sw = __ldg(S);
-  const bool verify = (A.flags & SPD_FUSE_VERIFY) != 0;
+  const spdvjp::Ctx x{&A.vg, &A.p, A.flags, A.model_step, __ldg(S)};
+  spdgen::DiffParams<float> g;
+  g.psmin = A.p.psmin; g.trcnv = A.p.trcnv; g.rhil = A.p.rhil; g.rhbl = A.p.rhbl;
+  g.entmax = A.p.entmax; g.smf = A.p.smf; g.trlsc = A.p.trlsc; g.rhlsc = A.p.rhlsc;
+  g.drhlsc = A.p.drhlsc; g.rhblsc = A.p.rhblsc; g.albcl = A.p.albcl; g.albcls = A.p.albcls;
   float pacc[SPD_NUM_DIFF_PARAMS];
 #pragma unroll
   for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] = 0.0f;
-  for (int c = gtid; c < C; c += nthr) {
-    tp.n = 0;
-    auto leaf = [&](float v) { return AF(v, tp.leaf(), &tp); };
-    spdgen::DiffParams<AF> g;
-    g.psmin = leaf(A.p.psmin); g.trcnv = leaf(A.p.trcnv); g.rhil = leaf(A.p.rhil);
-    g.rhbl = leaf(A.p.rhbl); g.entmax = leaf(A.p.entmax); g.smf = leaf(A.p.smf);
-    g.trlsc = leaf(A.p.trlsc); g.rhlsc = leaf(A.p.rhlsc); g.drhlsc = leaf(A.p.drhlsc);
-    g.rhblsc = leaf(A.p.rhblsc); g.albcl = leaf(A.p.albcl); g.albcls = leaf(A.p.albcls);
-    spdgen::ColumnIn<AF, float> x;
-    AF qraw[KX];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
+    spdgen::ColumnIn<float, float> xi;
+    float ct_t[KX], ct_q[KX];
+#pragma unroll 1
     for (int k = 0; k < KX; ++k) {
       const size_t i = (size_t)k * C + c;
-      x.t[k] = leaf(__ldg(in.temperature + i));
-      qraw[k] = leaf(__ldg(in.specific_humidity + i));
-      // verify_state (physics_interface.py:316): where(q < 0, 0, q)
-      x.q[k] = (verify && qraw[k].v < 0.0f) ? AF(0.0f) : qraw[k];
-      x.phi[k] = leaf(__ldg(in.geopotential + i));
+      xi.t[k] = __ldg(in.temperature + i);
+      xi.q[k] = __ldg(in.specific_humidity + i);
+      xi.phi[k] = __ldg(in.geopotential + i);
+      ct_t[k] = __ldg(ct.temperature + i);
+      ct_q[k] = __ldg(ct.specific_humidity + i);
     }
-    x.psa = leaf(__ldg(in.normalized_surface_pressure + c));
-    x.u_low = leaf(__ldg(in.u_wind + (size_t)(KX - 1) * C + c));
-    x.v_low = leaf(__ldg(in.v_wind + (size_t)(KX - 1) * C + c));
-    x.sst = __ldg(in.sea_surface_temperature + c);
-    x.stl = __ldg(in.stl_am + c);
-    x.soilw = __ldg(in.soilw_am + c);
-    x.snowc = __ldg(in.snowc_am + c);
-    x.sice = __ldg(in.sice_am + c);
-    x.alb0 = __ldg(in.alb0 + c);
-    x.fmask = __ldg(in.fmask + c);
-    x.orog = __ldg(in.orog + c);
-    x.phis0 = __ldg(in.phis0 + c);
+    const size_t lo = (size_t)(KX - 1) * C + c;
+    xi.psa = __ldg(in.normalized_surface_pressure + c);
+    xi.u_low = __ldg(in.u_wind + lo);
+    xi.v_low = __ldg(in.v_wind + lo);
+    xi.sst = __ldg(in.sea_surface_temperature + c);
+    xi.stl = __ldg(in.stl_am + c);
+    xi.soilw = __ldg(in.soilw_am + c);
+    xi.snowc = __ldg(in.snowc_am + c);
+    xi.sice = __ldg(in.sice_am + c);
+    xi.alb0 = __ldg(in.alb0 + c);
+    xi.fmask = __ldg(in.fmask + c);
+    xi.orog = __ldg(in.orog + c);
+    xi.phis0 = __ldg(in.phis0 + c);
     const ZonalRow z = table[c % A.il];
-    x.fsol = z.fsol; x.ozupp = z.ozupp; x.ozone = z.ozone; x.zenit = z.zenit;
-    x.stratz = z.stratz; x.sqrt_coa = z.sqrt_coa;
-    spdgen::ColumnOut<AF> o;
-    spdgen::column_generic<KX, AF, float>(A.vg, A.p, g, A.flags, A.model_step, A.ablco2, Sw, x,
-                                          o);
-    for (int k = 0; k < KX; ++k) {
-      AF dq = o.dq[k];
-      if (verify) {  // verify_tendencies (physics_interface.py:334-340)
-        dq = (qraw[k].v + A.dt_seconds * dq.v >= 0.0f) ? dq : -qraw[k] / A.dt_seconds;
-      }
-      if (A.q_tend_scale != 1.0f) dq = dq * A.q_tend_scale;
-      const size_t i = (size_t)k * C + c;
-      tp.seed(o.dt[k].i, __ldg(ct.temperature + i));
-      tp.seed(dq.i, __ldg(ct.specific_humidity + i));
-    }
-    tp.seed(o.du_low.i, __ldg(ct.u_wind + (size_t)(KX - 1) * C + c));
-    tp.seed(o.dv_low.i, __ldg(ct.v_wind + (size_t)(KX - 1) * C + c));
-    tp.reverse();
+    xi.fsol = z.fsol; xi.ozupp = z.ozupp; xi.ozone = z.ozone; xi.zenit = z.zenit;
+    xi.stratz = z.stratz; xi.sqrt_coa = z.sqrt_coa;
+    spdvjp::Bar<KX, float> b;
+    spdvjp::column_vjp<KX, float>(x, g, A.ablco2, A.dt_seconds, A.q_tend_scale, xi, ct_t, ct_q,
+                                  __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b);
+#pragma unroll 1
     for (int k = 0; k < KX; ++k) {
       const size_t i = (size_t)k * C + c;
-      gr.temperature[i] = tp.grad(x.t[k].i);
-      gr.specific_humidity[i] = tp.grad(qraw[k].i);
-      gr.geopotential[i] = tp.grad(x.phi[k].i);
-      gr.u_wind[i] = (k == KX - 1) ? tp.grad(x.u_low.i) : 0.0f;
-      gr.v_wind[i] = (k == KX - 1) ? tp.grad(x.v_low.i) : 0.0f;
+      gr.temperature[i] = b.t[k];
+      gr.specific_humidity[i] = b.q[k];
+      gr.geopotential[i] = b.phi[k];
+      gr.u_wind[i] = (k == KX - 1) ? b.u : 0.0f;
+      gr.v_wind[i] = (k == KX - 1) ? b.v : 0.0f;
     }
-    gr.normalized_surface_pressure[c] = tp.grad(x.psa.i);
-    const int pidx[SPD_NUM_DIFF_PARAMS] = {g.psmin.i, g.trcnv.i, g.rhil.i,   g.rhbl.i,
-                                           g.entmax.i, g.smf.i,   g.trlsc.i,  g.rhlsc.i,
-                                           g.drhlsc.i, g.rhblsc.i, g.albcl.i, g.albcls.i};
+    gr.normalized_surface_pressure[c] = b.psa;
 #pragma unroll
-    for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] += tp.grad(pidx[j]);
-    if (tp.overflow) atomicOr(status, 1u);
+    for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] += b.par[j];
   }
   // parameter gradients: warp, then block, then one atomic per block and parameter
-  __shared__ float red[kBlock / 32][SPD_NUM_DIFF_PARAMS];
+  __shared__ float red[kAdjBlock / 32][SPD_NUM_DIFF_PARAMS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) {
@@ -157,7 +105,7 @@ __global__ void __launch_bounds__(kBlock) adjoint_kernel(const VjpArgs A, const 
   __syncthreads();
   if (threadIdx.x < SPD_NUM_DIFF_PARAMS) {
     float v = 0.0f;
-    for (int w = 0; w < kBlock / 32; ++w) v += red[w][threadIdx.x];
+    for (int w = 0; w < kAdjBlock / 32; ++w) v += red[w][threadIdx.x];
     atomicAdd(gr.params + threadIdx.x, v);
   }
 }
@@ -165,17 +113,13 @@ __global__ void __launch_bounds__(kBlock) adjoint_kernel(const VjpArgs A, const 
 template <int KX>
 static int launch_vjp(const VjpArgs& A, const Consts& K, const spd_inputs_t& in,
                       const spd_cotangents_t& ct, const spd_grads_t& gr, char* scratch,
-                      const VjpLayout& L, cudaStream_t st) {
+                      cudaStream_t st) {
   uint32_t* S = reinterpret_cast<uint32_t*>(scratch);
-  uint32_t* status = S + 1;
-  ZonalRow* table = reinterpret_cast<ZonalRow*>(scratch + L.table);
+  ZonalRow* table = reinterpret_cast<ZonalRow*>(scratch + kAdjHeader);
   const int grid_a = (std::max(K.C, K.il) + kBlock - 1) / kBlock;
   cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
-  adjoint_kernel<KX><<<L.nthreads / kBlock, kBlock, 0, st>>>(
-      A, in, ct, gr, S, table, reinterpret_cast<int32_t*>(scratch + L.ia),
-      reinterpret_cast<int32_t*>(scratch + L.ib), reinterpret_cast<float*>(scratch + L.pa),
-      reinterpret_cast<float*>(scratch + L.pb), reinterpret_cast<float*>(scratch + L.adj),
-      status);
+  const int grid = (A.C + kAdjBlock - 1) / kAdjBlock;
+  adjoint_kernel<KX><<<grid, kAdjBlock, 0, st>>>(A, in, ct, gr, S, table);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
@@ -185,7 +129,7 @@ extern "C" {
 
 size_t spd_vjp_scratch_bytes(const spd_desc_t* desc) {
   if (!desc || desc->ix <= 0 || desc->il <= 0) return 0;
-  return spd::vjp_layout(desc).total;
+  return spd::vjp_scratch(desc);
 }
 
 int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
@@ -204,8 +148,8 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
                        grads->geopotential, grads->normalized_surface_pressure, grads->params};
   for (const void* p : req)
     if (!p) return SPD_ERR_NULL;
-  const VjpLayout L = vjp_layout(desc);
-  if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) || scratch_bytes < L.total)
+  if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) ||
+      scratch_bytes < vjp_scratch(desc))
     return SPD_ERR_SCRATCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const Consts K = make_consts(desc, vgrid, params);
@@ -217,7 +161,6 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
   A.model_step = desc->model_step;
   A.C = desc->ix * desc->il;
   A.il = desc->il;
-  A.cap = L.cap;
   A.ablco2 = D.ablco2;
   A.dt_seconds = desc->dt_seconds;
   A.q_tend_scale = desc->q_tend_scale;
@@ -226,9 +169,9 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
   if (cudaMemsetAsync(grads->params, 0, SPD_NUM_DIFF_PARAMS * sizeof(float), st) != cudaSuccess)
     return SPD_ERR_CUDA;
   switch (desc->kx) {
-    case 7: return launch_vjp<7>(A, K, *in, *ct, *grads, sc, L, st);
-    case 8: return launch_vjp<8>(A, K, *in, *ct, *grads, sc, L, st);
-    case 16: return launch_vjp<16>(A, K, *in, *ct, *grads, sc, L, st);
+    case 7: return launch_vjp<7>(A, K, *in, *ct, *grads, sc, st);
+    case 8: return launch_vjp<8>(A, K, *in, *ct, *grads, sc, st);
+    case 16: return launch_vjp<16>(A, K, *in, *ct, *grads, sc, st);
     default: return SPD_ERR_KX;
   }
 }

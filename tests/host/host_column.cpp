@@ -1,11 +1,12 @@
 // Host build of the generic column physics (jax-gcm_b200/csrc/speedy_generic.h) for the CPU
-// tests: forward in float32 and float64, and the reverse-mode VJP in float64 with the tape in
-// host memory.  Test infrastructure only.
+// tests: forward in float32 and float64, the reverse-mode VJP with the tape in host memory, and
+// the hand-written reverse pass (jax-gcm_b200/csrc/speedy_vjp.h).  Test infrastructure only.
 #include <cmath>
 #include <cstdint>
 #include <vector>
 
 #include "speedy_generic.h"
+#include "speedy_vjp.h"
 
 using spdad::Adj;
 using spdad::TapeT;
@@ -73,7 +74,8 @@ template <int KX, class T = double>
 static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h,
                const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv,
                double* g_t, double* g_q, double* g_phi, double* g_psa, double* g_u,
-               double* g_v, double* g_params) {
+               double* g_v, double* g_params, double dt_seconds = 1800.0,
+               double q_tend_scale = 1.0) {
   typedef Adj<T> A;
   const int cap = 1 << 20;
   std::vector<int32_t> ia(cap), ib(cap);
@@ -87,9 +89,13 @@ static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h
   g.albcl = leaf(p.albcl); g.albcls = leaf(p.albcls);
   spdgen::ColumnIn<A, T> in;
   fill_in(h, in);
+  const bool verify = (h.flags & SPD_FUSE_VERIFY) != 0;
+  A qraw[KX];
   for (int k = 0; k < KX; ++k) {
     in.t[k] = leaf(h.t[k]);
-    in.q[k] = leaf(h.q[k]);
+    qraw[k] = leaf(h.q[k]);
+    // verify_state (physics_interface.py:316): where(q < 0, 0, q)
+    in.q[k] = (verify && qraw[k].v < T(0)) ? A(T(0)) : qraw[k];
     in.phi[k] = leaf(h.phi[k]);
   }
   in.psa = leaf(h.psa);
@@ -98,15 +104,19 @@ static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h
   spdgen::ColumnOut<A> o;
   spdgen::column_generic<KX, A, T>(vg, p, g, h.flags, h.model_step, T(h.ablco2), h.S, in, o);
   for (int k = 0; k < KX; ++k) {
+    A dq = o.dq[k];
+    if (verify)  // verify_tendencies (physics_interface.py:334-340)
+      dq = (qraw[k].v + T(dt_seconds) * dq.v >= T(0)) ? dq : -qraw[k] / T(dt_seconds);
+    if (q_tend_scale != 1.0) dq = dq * T(q_tend_scale);
     tp.seed(o.dt[k].i, T(ct_dt[k]));
-    tp.seed(o.dq[k].i, T(ct_dq[k]));
+    tp.seed(dq.i, T(ct_dq[k]));
   }
   tp.seed(o.du_low.i, T(ct_du));
   tp.seed(o.dv_low.i, T(ct_dv));
   tp.reverse();
   for (int k = 0; k < KX; ++k) {
     g_t[k] = tp.grad(in.t[k].i);
-    g_q[k] = tp.grad(in.q[k].i);
+    g_q[k] = tp.grad(qraw[k].i);
     g_phi[k] = tp.grad(in.phi[k].i);
   }
   *g_psa = tp.grad(in.psa.i);
@@ -118,7 +128,67 @@ static int vjp(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h
   return tp.overflow ? -1 : tp.n;
 }
 
+// The hand-written reverse pass, same arguments as vjp.
+template <int KX, class T = double>
+static int vjp_hand(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h,
+                    const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv,
+                    double* g_t, double* g_q, double* g_phi, double* g_psa, double* g_u,
+                    double* g_v, double* g_params, double dt_seconds = 1800.0,
+                    double q_tend_scale = 1.0) {
+  spdgen::DiffParams<T> g;
+  fill_params(p, g);
+  spdgen::ColumnIn<T, T> in;
+  fill_in(h, in);
+  spdvjp::Ctx x{&vg, &p, h.flags, h.model_step, h.S};
+  T ct[2][KX];
+  for (int k = 0; k < KX; ++k) {
+    ct[0][k] = T(ct_dt[k]);
+    ct[1][k] = T(ct_dq[k]);
+  }
+  spdvjp::Bar<KX, T> b;
+  spdvjp::column_vjp<KX, T>(x, g, T(h.ablco2), T(dt_seconds), T(q_tend_scale), in, ct[0], ct[1],
+                            T(ct_du), T(ct_dv), b);
+  for (int k = 0; k < KX; ++k) {
+    g_t[k] = b.t[k];
+    g_q[k] = b.q[k];
+    g_phi[k] = b.phi[k];
+  }
+  *g_psa = b.psa;
+  *g_u = b.u;
+  *g_v = b.v;
+  for (int j = 0; j < 12; ++j) g_params[j] = b.par[j];
+  return 1;
+}
+
 extern "C" {
+
+#define HC_VJP_ARGS                                                                        \
+  const spd_vgrid_t *vg, const spd_params_t *p, const HostColumn *h, const double *ct_dt, \
+      const double *ct_dq, double ct_du, double ct_dv, double *g_t, double *g_q,          \
+      double *g_phi, double *g_psa, double *g_u, double *g_v, double *g_params,           \
+      double dt_seconds, double q_tend_scale
+#define HC_VJP_PASS                                                                      \
+  *vg, *p, *h, ct_dt, ct_dq, ct_du, ct_dv, g_t, g_q, g_phi, g_psa, g_u, g_v, g_params, \
+      dt_seconds, q_tend_scale
+
+// mode: 0 tape float64, 1 tape float32, 2 hand float64, 3 hand float32
+int hc_vjp_any(int mode, HC_VJP_ARGS) {
+  switch (h->kx * 4 + mode) {
+    case 7 * 4 + 0: return vjp<7, double>(HC_VJP_PASS);
+    case 7 * 4 + 1: return vjp<7, float>(HC_VJP_PASS);
+    case 7 * 4 + 2: return vjp_hand<7, double>(HC_VJP_PASS);
+    case 7 * 4 + 3: return vjp_hand<7, float>(HC_VJP_PASS);
+    case 8 * 4 + 0: return vjp<8, double>(HC_VJP_PASS);
+    case 8 * 4 + 1: return vjp<8, float>(HC_VJP_PASS);
+    case 8 * 4 + 2: return vjp_hand<8, double>(HC_VJP_PASS);
+    case 8 * 4 + 3: return vjp_hand<8, float>(HC_VJP_PASS);
+    case 16 * 4 + 0: return vjp<16, double>(HC_VJP_PASS);
+    case 16 * 4 + 1: return vjp<16, float>(HC_VJP_PASS);
+    case 16 * 4 + 2: return vjp_hand<16, double>(HC_VJP_PASS);
+    case 16 * 4 + 3: return vjp_hand<16, float>(HC_VJP_PASS);
+  }
+  return -2;
+}
 
 int hc_vjp32(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h,
              const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv, double* g_t,

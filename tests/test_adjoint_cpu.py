@@ -1,5 +1,6 @@
-"""The generic column restatement (jax-gcm_b200/csrc/speedy_generic.h) and its reverse-mode
-VJP, built for the host from the same source (tests/host/host_column.cpp):
+"""The generic column restatement (jax-gcm_b200/csrc/speedy_generic.h), its reverse-mode tape
+VJP, and the hand-written reverse pass (jax-gcm_b200/csrc/speedy_vjp.h, the device adjoint),
+built for the host from the same sources (tests/host/host_column.cpp):
 
 * the generic forward agrees with the oracle (float32 at the parity bar, float64 to 1e-9 when
   both see the same float32-rounded tables);
@@ -7,7 +8,10 @@ VJP, built for the host from the same source (tests/host/host_column.cpp):
   h = 1e-3 relative, and along random state directions with h = 1e-5 relative (the column
   physics is piecewise smooth -- max/min/where at many thresholds -- and a 1e-3 relative step
   of the state crosses one of those kinks in about half the columns; 1e-5 stays on one piece
-  in almost all).
+  in almost all);
+* the hand-written reverse pass equals the tape VJP in float64 to 1e-9 (the same derivative,
+  accumulated in another order) for every flag combination, with the fused verify step, and
+  in float32 is as close to float64 as the float32 tape is.
 """
 import ctypes as C
 import importlib
@@ -51,6 +55,7 @@ def build_host(out):
     lib.hc_vjp.argtypes = [C.c_void_p, C.c_void_p, P(HostColumn), d, d, C.c_double,
                            C.c_double, d, d, d, d, d, d, d]
     lib.hc_vjp32.argtypes = lib.hc_vjp.argtypes
+    lib.hc_vjp_any.argtypes = [C.c_int] + lib.hc_vjp.argtypes + [C.c_double, C.c_double]
     return lib
 
 
@@ -261,3 +266,85 @@ def test_vjp_parameter_gradients_match_central_differences(pkg, host, h_rel, min
         if abs(fd - gsum[n]) <= 2e-3 * max(abs(fd), abs(gsum[n])) + 1e-12:
             good += 1
     assert good >= min_good, good
+
+
+VJP_TAPE64, VJP_TAPE32, VJP_HAND64, VJP_HAND32 = 0, 1, 2, 3
+SPD_LFLUXLAND, SPD_LSCASYM, SPD_LSKINEB, SPD_FUSE_VERIFY = 1, 2, 4, 16
+
+
+def vjp_any(host, mode, vg, pr, h, ct, dt_seconds=1800.0, q_tend_scale=1.0):
+    ct_t, ct_q, ct_u, ct_v = ct
+    arr = lambda: (C.c_double * 16)()
+    gt, gq, gphi, gp = arr(), arr(), arr(), (C.c_double * 12)()
+    gpsa, gu, gv = C.c_double(), C.c_double(), C.c_double()
+    n = host.hc_vjp_any(mode, C.byref(vg), C.byref(pr), C.byref(h), (C.c_double * 16)(*ct_t),
+                        (C.c_double * 16)(*ct_q), ct_u, ct_v, gt, gq, gphi, C.byref(gpsa),
+                        C.byref(gu), C.byref(gv), gp, dt_seconds, q_tend_scale)
+    assert n > 0, n
+    kx = h.kx
+    return dict(t=np.array(gt[:kx]), q=np.array(gq[:kx]), phi=np.array(gphi[:kx]),
+                psa=np.array([gpsa.value]), u=np.array([gu.value]), v=np.array([gv.value]),
+                params=np.array(gp[:]))
+
+
+FLAG_SETS = [SPD_LFLUXLAND | SPD_LSCASYM | SPD_LSKINEB, 0, SPD_LFLUXLAND | SPD_LSKINEB,
+             SPD_LFLUXLAND | SPD_LSCASYM, SPD_LFLUXLAND | SPD_LSCASYM | SPD_LSKINEB | SPD_FUSE_VERIFY]
+
+
+@pytest.mark.parametrize("kx", [7, 8, 16])
+def test_hand_reverse_pass_equals_tape_vjp_float64(pkg, host, kx):
+    """Every gradient of the hand-written reverse pass against the tape's, columnwise, over
+    land/sea/ice columns, both shortwave states, every flag set; with the fused verify step a
+    third of the columns get a negative humidity and the humidity scale is 0.9."""
+    inst = pkg.synthetic.land_instance(31 + kx, 16, 8, kx, sst_noise=1.5)
+    vg, pr = structs(pkg, inst)
+    tend, data, S = run_oracle(inst)
+    rng = np.random.default_rng(kx)
+    worst = 0.0
+    for flags in FLAG_SETS:
+        verify = bool(flags & SPD_FUSE_VERIFY)
+        for ms in (0, 1):
+            for i in range(0, 16, 2):
+                for j in range(8):
+                    h = column_of(inst, data, S, i, j, flags)
+                    h.model_step = ms
+                    if verify and (i + j) % 3 == 0:
+                        h.q[2] = -abs(h.q[2]) * 0.1 - 1e-4
+                    ct = (list(rng.normal(size=16)), list(rng.normal(size=16)),
+                          float(rng.normal()), float(rng.normal()))
+                    sc = 0.9 if verify else 1.0
+                    a = vjp_any(host, VJP_TAPE64, vg, pr, h, ct, 1800.0, sc)
+                    b = vjp_any(host, VJP_HAND64, vg, pr, h, ct, 1800.0, sc)
+                    for k in a:
+                        e = np.max(np.abs(a[k] - b[k])) / max(np.max(np.abs(a[k])), 1e-300)
+                        assert e <= 1e-9, (flags, ms, i, j, k, e)
+                        worst = max(worst, e)
+    print("worst relative difference", worst)
+
+
+@pytest.mark.parametrize("kx", [8, 16])
+def test_hand_reverse_pass_float32_accuracy(pkg, host, kx):
+    """Normwise over 128 columns, the float32 hand pass is within max(2e-5, 3x the float32
+    tape's own error) of the float64 tape."""
+    inst = pkg.synthetic.land_instance(51 + kx, 16, 8, kx)
+    vg, pr = structs(pkg, inst)
+    tend, data, S = run_oracle(inst)
+    rng = np.random.default_rng(3)
+    G = {m: {} for m in (VJP_TAPE64, VJP_TAPE32, VJP_HAND32)}
+    for i in range(16):
+        for j in range(8):
+            h = column_of(inst, data, S, i, j, _flags(inst))
+            ct = (list(rng.normal(size=16)), list(rng.normal(size=16)), float(rng.normal()),
+                  float(rng.normal()))
+            for m in G:
+                for k, v in vjp_any(host, m, vg, pr, h, ct).items():
+                    G[m].setdefault(k, []).append(v)
+    for k in ("t", "q", "phi", "psa", "u", "v"):
+        ref = np.array(G[VJP_TAPE64][k])
+        sc = np.max(np.abs(ref))
+        own = np.max(np.abs(np.array(G[VJP_TAPE32][k]) - ref)) / sc
+        hand = np.max(np.abs(np.array(G[VJP_HAND32][k]) - ref)) / sc
+        assert hand <= max(2e-5, 3 * own), (k, hand, own)
+    ref = np.array(G[VJP_TAPE64]["params"]).sum(0)
+    hand = np.array(G[VJP_HAND32]["params"]).sum(0)
+    assert np.all(np.abs(hand - ref) <= 1e-4 * np.max(np.abs(ref)))
