@@ -160,7 +160,103 @@ static int vjp_hand(const spd_vgrid_t& vg, const spd_params_t& p, const HostColu
   return 1;
 }
 
+// Float64 rollout of one column as a single-column instance (its own cloud-top level set at
+// every step): the fused step (verify_state, physics, verify_tendencies) and the explicit
+// update x += dt * tendency for T, q and the lowest-level winds.  x0: t[16], q[16], phi[16],
+// psa, u, v.  ct: t[16], q[16], u, v.  Returns <ct, x_N>; with grad non-null, also the
+// gradient of that with respect to x0 (same layout as x0) and the 12 parameters, by storing
+// every state and applying the hand-written reverse pass from the last step to the first.
+template <int KX>
+static double rollout(const spd_vgrid_t& vg, const spd_params_t& p, const HostColumn& h,
+                      const double* x0, int nsteps, double dt, const double* ct, double* grad,
+                      double* gpar) {
+  typedef spdgen::ColumnIn<double, double> In;
+  std::vector<In> xs(nsteps + 1);
+  fill_in(h, xs[0]);
+  for (int k = 0; k < KX; ++k) {
+    xs[0].t[k] = x0[k];
+    xs[0].q[k] = x0[16 + k];
+    xs[0].phi[k] = x0[32 + k];
+  }
+  xs[0].psa = x0[48];
+  xs[0].u_low = x0[49];
+  xs[0].v_low = x0[50];
+  std::vector<uint32_t> S(nsteps);
+  spdgen::DiffParams<double> g;
+  fill_params(p, g);
+  const uint32_t fl = h.flags & ~(uint32_t)SPD_FUSE_VERIFY;
+  for (int n = 0; n < nsteps; ++n) {
+    In xu = xs[n];
+    for (int k = 0; k < KX; ++k) xu.q[k] = xs[n].q[k] < 0.0 ? 0.0 : xs[n].q[k];
+    spdgen::ColumnOut<double> o;
+    spdgen::column_generic<KX, double, double>(vg, p, g, fl, h.model_step + n, h.ablco2, 0u,
+                                               xu, o);
+    const int ic = o.icltop < 0 ? 0 : (o.icltop > KX - 1 ? KX - 1 : o.icltop);
+    S[n] = 1u << ic;
+    spdgen::column_generic<KX, double, double>(vg, p, g, fl, h.model_step + n, h.ablco2, S[n],
+                                               xu, o);
+    xs[n + 1] = xs[n];
+    for (int k = 0; k < KX; ++k) {
+      double dq = o.dq[k];
+      if (!(xs[n].q[k] + dt * dq >= 0.0)) dq = -xs[n].q[k] / dt;
+      xs[n + 1].t[k] += dt * o.dt[k];
+      xs[n + 1].q[k] += dt * dq;
+    }
+    xs[n + 1].u_low += dt * o.du_low;
+    xs[n + 1].v_low += dt * o.dv_low;
+  }
+  const In& xN = xs[nsteps];
+  double loss = ct[32] * xN.u_low + ct[33] * xN.v_low;
+  for (int k = 0; k < KX; ++k) loss += ct[k] * xN.t[k] + ct[16 + k] * xN.q[k];
+  if (!grad) return loss;
+  double xt[KX], xq[KX], phib[KX] = {}, xu_ = ct[32], xv_ = ct[33], psab = 0.0, par[12] = {};
+  for (int k = 0; k < KX; ++k) {
+    xt[k] = ct[k];
+    xq[k] = ct[16 + k];
+  }
+  for (int n = nsteps - 1; n >= 0; --n) {
+    spdvjp::Ctx x{&vg, &p, h.flags | (uint32_t)SPD_FUSE_VERIFY, h.model_step + n, S[n]};
+    double ctt[KX], ctq[KX];
+    for (int k = 0; k < KX; ++k) {
+      ctt[k] = dt * xt[k];
+      ctq[k] = dt * xq[k];
+    }
+    spdvjp::Bar<KX, double> b;
+    spdvjp::column_vjp<KX, double>(x, g, h.ablco2, dt, 1.0, xs[n], ctt, ctq, dt * xu_, dt * xv_,
+                                   b);
+    for (int k = 0; k < KX; ++k) {
+      xt[k] += b.t[k];
+      xq[k] += b.q[k];
+      phib[k] += b.phi[k];
+    }
+    xu_ += b.u;
+    xv_ += b.v;
+    psab += b.psa;
+    for (int j = 0; j < 12; ++j) par[j] += b.par[j];
+  }
+  for (int k = 0; k < KX; ++k) {
+    grad[k] = xt[k];
+    grad[16 + k] = xq[k];
+    grad[32 + k] = phib[k];
+  }
+  grad[48] = psab;
+  grad[49] = xu_;
+  grad[50] = xv_;
+  for (int j = 0; j < 12; ++j) gpar[j] = par[j];
+  return loss;
+}
+
 extern "C" {
+
+double hc_rollout(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h,
+                  const double* x0, int nsteps, double dt, const double* ct, double* grad,
+                  double* gpar) {
+  switch (h->kx) {
+    case 8: return rollout<8>(*vg, *p, *h, x0, nsteps, dt, ct, grad, gpar);
+    case 16: return rollout<16>(*vg, *p, *h, x0, nsteps, dt, ct, grad, gpar);
+  }
+  return 0.0;
+}
 
 #define HC_VJP_ARGS                                                                        \
   const spd_vgrid_t *vg, const spd_params_t *p, const HostColumn *h, const double *ct_dt, \
