@@ -44,6 +44,9 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sections", default="t425,adjoint,serving",
+                    help="extra single-GPU sections: t425, adjoint, serving (comma list, or none)")
+    ap.add_argument("--serving-requests", type=int, default=400)
     return ap.parse_args()
 
 
@@ -170,12 +173,14 @@ def run_b200(args):
                            runs[0][4])
         ens.autotune()
 
-        def step():
-            ens.forward()
+        def step(marker=None):
+            ens.forward(marker=marker)
 
         launches_per_step = 2
     else:
-        step = step_plain
+        def step(marker=None):
+            step_plain()
+
         launches_per_step = 2 * len(runs)
 
     def barrier():
@@ -202,13 +207,42 @@ def run_b200(args):
             ms = float(t.item())
         return ms
 
+    # The timed region: K steps between two events, with a marker event between the pre-pass
+    # and the column pass of every step (batched mode) so the column kernel is timed alone.
+    marks = [(primed_event(), primed_event(), primed_event()) for _ in range(args.steps)]
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
     clocks = ClockSampler(dev.index)
     clocks.start()
     time.sleep(0.3)
-    total_ms = timed(step, args.steps, args.warmup)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for (a, m, b) in marks:
+        if ens is not None:
+            a.record()
+            step(marker=m)
+            b.record()
+        else:
+            step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
     clk = clocks.stop()
+    total_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
     ms_step = total_ms / args.steps
+    col_ms = pre_ms = None
+    if ens is not None:
+        col_ms = sum(m.elapsed_time(b) for (a, m, b) in marks) / args.steps
+        pre_ms = sum(a.elapsed_time(m) for (a, m, b) in marks) / args.steps
     value = cols * world / (ms_step / 1e3)
+    grid_blocks = ens.grid_blocks if ens is not None else None
     plain = None
     if args.mode == "batched" and not args.no_plain:
         pms = timed(step_plain, args.steps, args.warmup) / args.steps
@@ -216,16 +250,20 @@ def run_b200(args):
                  "launches_per_step": 2 * len(runs),
                  "batched_over_plain": round(pms / ms_step, 2)}
 
-    # roofline of the fused forward (cloud-top pre-pass + column kernel), per launch pair
+    # roofline of the dominant kernel (the column pass): the algorithmic bytes of one forward
+    # (every input read once, every output written once) over its own event-timed duration
     peak, peak_kind = load_peaks()
-    achieved = bytes_step / (ms_step / 1e3) / 1e9
+    kern_ms = col_ms if col_ms is not None else ms_step
+    achieved = bytes_step / (kern_ms / 1e3) / 1e9
     traffic = NCU_TRAFFIC_PER_COLUMN.get(args.workload)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "kernel": ("ensemble_prepass + ensemble_columns (one step)" if ens is not None
-                           else "cloudtop_prepass + column_kernel (one forward)"),
-                "algorithmic_bytes_per_step": bytes_step,
-                "traffic": (traffic * cols if traffic else None)}
+                "kernel": ("ensemble_columns" if ens is not None
+                           else "cloudtop_prepass + column_kernel (one forward per member)"),
+                "kernel_ms": round(kern_ms, 4),
+                "prepass_ms": (round(pre_ms, 4) if pre_ms is not None else None),
+                "algorithmic_bytes_per_launch": bytes_step,
+                "traffic": (round(traffic * cols) if traffic else None)}
 
     # end to end through the public API with host buffers (pinned), H2D + D2H timed
     e2e = None
@@ -271,6 +309,18 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(members)
 
+    sections = {}
+    wanted = [x for x in args.sections.split(",") if x and x != "none"]
+    if world == 1:
+        del runs, ens
+        torch.cuda.empty_cache()
+        if "t425" in wanted:
+            sections["t425"] = t425_section(pkg, dev, peak, peak_kind)
+        if "adjoint" in wanted:
+            sections["adjoint"] = adjoint_section(pkg, dev)
+        if "serving" in wanted:
+            sections["serving"] = serving_section(pkg, dev, args.serving_requests)
+
     if rank == 0:
         line = {"metric": "physics columns/s", "value": round(value, 1), "unit": "columns/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -279,11 +329,163 @@ def run_b200(args):
                 "data": "synthetic (seeded generators with the workload's shapes and distributions)",
                 "config": workload_config(args.workload, members, args.mode),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-                "plain": plain, "grid_blocks": (ens.grid_blocks if ens is not None else None),
+                "plain": plain, "grid_blocks": grid_blocks,
                 "gpu_launches": launches_per_step * args.steps}
+        line.update(sections)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def primed_event():
+    """A timing event whose CUDA event exists (torch creates it on the first record)."""
+    import torch
+    e = torch.cuda.Event(enable_timing=True)
+    e.record()
+    return e
+
+
+def event_ms(fn, reps, warmup=3):
+    """Mean device milliseconds of fn() over reps calls (events on the current stream)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def t425_section(pkg, dev, peak, peak_kind):
+    """T425 (1280x640, 16 levels): the plain drop-in call, its column kernel timed alone, and 24
+    consecutive calls captured in one CUDA graph."""
+    import torch
+    inst = pkg.synthetic.t425_instance()
+    st, fo, ge, da = pkg.instance_to_device(inst, dev)
+    phys = pkg.SpeedyPhysics(diagnostics=False)
+    e3 = lambda: torch.empty((inst.kx, inst.ix, inst.il), dtype=torch.float32, device=dev)
+    e2 = lambda: torch.empty((inst.ix, inst.il), dtype=torch.float32, device=dev)
+    out = dict(u_wind=e3(), v_wind=e3(), temperature=e3(), specific_humidity=e3(),
+               precnv=e2(), precls=e2())
+    call = lambda marker=None: phys.compute_tendencies(st, fo, ge, da, out=out, marker=marker)
+    reps = 24
+    marks = [(primed_event(), primed_event(), primed_event()) for _ in range(reps)]
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    for (a, m, b) in marks:
+        a.record()
+        call(marker=m)
+        b.record()
+    torch.cuda.synchronize()
+    call_ms = sum(a.elapsed_time(b) for (a, m, b) in marks) / reps
+    col_ms = sum(m.elapsed_time(b) for (a, m, b) in marks) / reps
+    # 24 calls in one graph
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        call()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(24):
+            call()
+    graph_ms = event_ms(g.replay, 5, warmup=2) / 24
+    cols = inst.columns
+    nbytes = pkg.synthetic.fwd_bytes(inst.kx, cols)
+    bw = nbytes / (col_ms / 1e3) / 1e9
+    out_d = {"workload": "T425 1280x640, 16 levels, one instance", "columns": cols,
+             "algorithmic_bytes_per_call": nbytes,
+             "plain_call_ms": round(call_ms, 4), "column_kernel_ms": round(col_ms, 4),
+             "graph_24_calls_ms_per_call": round(graph_ms, 4),
+             "columns_per_s_plain": round(cols / (call_ms / 1e3), 1),
+             "columns_per_s_graph": round(cols / (graph_ms / 1e3), 1),
+             "column_kernel_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
+             "column_kernel_hbm_frac": round(bw / peak, 4)}
+    del g
+    return out_d
+
+
+def adjoint_section(pkg, dev):
+    """Adjoint at T42 (128x64 = 8,192 columns, 8 levels): one VJP call beside one forward call,
+    and the 48-step rollout VJP with checkpoints every 8 steps; plus the VJP at T170x16."""
+    import torch
+    res = {}
+    for label, (ix, il, kx) in (("t42_k8", (128, 64, 8)), ("t170_k16", (512, 256, 16))):
+        inst = pkg.synthetic.land_instance(42, ix, il, kx)
+        st, fo, ge, da = pkg.instance_to_device(inst, dev)
+        phys = pkg.SpeedyPhysics(diagnostics=False)
+        gen = torch.Generator(device=dev).manual_seed(0)
+        ct = pkg.PhysicsTendency(*(torch.randn(st.temperature.shape, generator=gen, device=dev)
+                                   for _ in range(4)))
+        vjp_ms = event_ms(lambda: pkg.adjoint.vjp(phys, st, fo, ge, da, ct), 20)
+        fwd_ms = event_ms(lambda: phys.compute_tendencies(st, fo, ge, da), 20)
+        r = {"columns": inst.columns, "vjp_ms": round(vjp_ms, 4), "forward_ms": round(fwd_ms, 4),
+             "vjp_columns_per_s": round(inst.columns / (vjp_ms / 1e3), 1),
+             "vjp_over_forward": round(vjp_ms / fwd_ms, 2)}
+        if label == "t42_k8":
+            roll_ms = event_ms(lambda: pkg.rollout.rollout_vjp(None, st, fo, ge, da, ct,
+                                                               nsteps=48, checkpoint_every=8),
+                               2, warmup=1)
+            r["rollout48_vjp_ms"] = round(roll_ms, 2)
+            r["rollout48_checkpoint_every"] = 8
+        res[label] = r
+    return res
+
+
+def serving_section(pkg, dev, n_requests):
+    """The request stream (Poisson, 200 req/s, 80/20 tendency/VJP, 1-32 members at T21-T170,
+    8 or 16 levels) under a 120 GB budget: continuous batching against the plain per-request
+    drop-in, and both at saturation (every request arriving at once)."""
+    import gc
+    import torch
+    S = pkg.serving
+    src = S.synthetic_source()
+    reqs = S.poisson_stream(seed=1, rate=200.0, n=n_requests)
+    sat = S.poisson_stream(seed=2, rate=0.0, n=max(50, n_requests // 4))
+    for r in reqs + sat:
+        for k in r.members:
+            src(k)
+    budget = 120 << 30
+    out = {"workload": "Poisson 200 req/s, 80/20 tendency/VJP, 1-32 members, T21-T170, 8/16 "
+                       "levels, 120 GB budget; member state resident before the stream",
+           "requests": n_requests}
+    for mode in ("batched", "plain"):
+        # the device pool is reserved once at startup, the size of the admission budget less
+        # the adjoint and forward scratch
+        be = S.CudaBackend(dev, mode=mode, reserve_bytes=budget - (1 << 30))
+        warm = S.Scheduler(be, src, budget, mode=mode)
+        warm.run([S.Request(S.TENDENCY, list(r.members)) for r in reqs[:8]] +
+                 [S.Request(S.VJP, list(r.members)) for r in reqs[:2]])
+        for label, stream in (("stream", reqs), ("saturation", sat)):
+            sch = S.Scheduler(be, src, budget, mode=mode)
+            # member state is resident before traffic arrives (a resident-state service)
+            sch.prefetch([k for r in stream for k in r.members])
+            fin = sch.run([S.Request(r.kind, list(r.members), r.arrival, r.seed) for r in stream],
+                          timeout_s=600)
+            st = S.latency_stats(fin)
+            st.update({k: round(v, 4) for k, v in S.overlap_stats(sch.items).items()})
+            st["launches"] = {k: v for k, v in sch.stats.items() if k.startswith("launches")}
+            st["uploads_during_run"] = sch.stats.get("uploads", 0)
+            st["prefetched_members"] = sch.stats.get("prefetched", 0)
+            st["peak_budget_bytes"] = sch.peak
+            out[f"{mode}_{label}"] = {k: (round(v, 3) if isinstance(v, float) else v)
+                                      for k, v in st.items()}
+            del sch, fin
+        # release this backend's pool before the next one reserves its own
+        del be, warm
+        gc.collect()
+        torch.cuda.empty_cache()
+    b, p = out["batched_stream"], out["plain_stream"]
+    out["p50_ms"], out["p99_ms"] = b["p50_ms"], b["p99_ms"]
+    out["plain_p50_ms"], out["plain_p99_ms"] = p["p50_ms"], p["p99_ms"]
+    out["saturation_columns_per_s"] = out["batched_saturation"]["columns_per_s"]
+    out["plain_saturation_columns_per_s"] = out["plain_saturation"]["columns_per_s"]
+    return out
 
 
 _MEMBER_CACHE = {}

@@ -130,6 +130,19 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
             const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
             size_t scratch_bytes, void* stream);
 
+/* Timing hook (no reference counterpart): spd_fwd, recording `event` (a cudaEvent_t, or NULL)
+ * on `stream` between the cloud-top pre-pass and the column kernel, so that a caller can time
+ * the two launches separately with events. */
+int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+                   const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
+                   size_t scratch_bytes, void* stream, void* event);
+
+/* Loads every kernel of the library on the current device (no reference counterpart).  CUDA
+ * loads modules lazily by default, and loading one while other kernels run waits for them;
+ * calling this once per device before latency-sensitive use keeps that wait out of the first
+ * launches. */
+int spd_preload(void);
+
 /* ----------------------------------------------------------------------------------------- */
 /* Adjoint (vector-Jacobian product) of the plain forward.                                    */
 /* Replaces jax.vjp of SpeedyPhysics.compute_tendencies (speedy_physics.py:88-127; the         */
@@ -211,6 +224,34 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
 /* Runs every member.  grid_blocks = 0 picks SMs x resident blocks; otherwise the persistent
  * grid size (the autotuner's knob). */
 int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device,
+                     const spd_plan_info_t* info, int grid_blocks, void* stream);
+
+/* Timing hook (no reference counterpart): spd_ensemble_fwd, recording `event` (a cudaEvent_t,
+ * or NULL) on `stream` between the pre-pass and the column pass. */
+int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
+                            const spd_plan_info_t* info, int grid_blocks, void* stream,
+                            void* event);
+
+/* Batched adjoint: the VJP of every member of a ragged ensemble in one pre-pass launch and one
+ * adjoint launch (no reference counterpart for the batching; per member it is spd_vjp).  Each
+ * member gives the same gradients as spd_vjp on it alone; its 12 parameter gradients are its
+ * own (grads.params of each member, zeroed by the call). */
+typedef struct {
+  spd_inputs_t in;
+  spd_cotangents_t ct;
+  spd_grads_t grads;
+  int32_t ix, il, cls, reserved;
+} spd_vjp_member_t;
+
+size_t spd_ensemble_vjp_plan_bytes(const spd_vjp_member_t* members, int nmembers);
+
+int spd_ensemble_vjp_plan(const spd_class_t* classes, int nclasses,
+                          const spd_vjp_member_t* members, int nmembers, void* plan_host,
+                          void* plan_device, size_t plan_bytes, spd_plan_info_t* info);
+
+/* grid_blocks = 0: one block per tile (short blocks, so the SMs turn over and kernels of a
+ * higher-priority stream get them quickly); otherwise a persistent grid of that many blocks. */
+int spd_ensemble_vjp(const spd_class_t* classes, int nclasses, void* plan_device,
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 
 /* ----------------------------------------------------------------------------------------- */

@@ -95,6 +95,11 @@ class Grads(C.Structure):
                                           "params")]
 
 
+class VjpMember(C.Structure):
+    _fields_ = [("inp", Inputs), ("ct", Cotangents), ("grads", Grads), ("ix", C.c_int32),
+                ("il", C.c_int32), ("cls", C.c_int32), ("reserved", C.c_int32)]
+
+
 DIFF_PARAM_NAMES = ["psmin", "trcnv", "rhil", "rhbl", "entmax", "smf", "trlsc", "rhlsc",
                     "drhlsc", "rhblsc", "albcl", "albcls"]
 
@@ -118,6 +123,8 @@ def _declare(lib):
     lib.spd_fwd.argtypes = [P(Desc), P(VGrid), P(Params), P(Inputs), P(Outputs), C.c_void_p,
                             C.c_size_t, C.c_void_p]
     lib.spd_fwd.restype = C.c_int
+    lib.spd_fwd_marked.argtypes = lib.spd_fwd.argtypes + [C.c_void_p]
+    lib.spd_fwd_marked.restype = C.c_int
     lib.spd_status_string.argtypes = [C.c_int]
     lib.spd_status_string.restype = C.c_char_p
     lib.spd_abi_version.argtypes = []
@@ -135,11 +142,23 @@ def _declare(lib):
     lib.spd_ensemble_fwd.argtypes = [P(Class), C.c_int, C.c_void_p, P(PlanInfo), C.c_int,
                                      C.c_void_p]
     lib.spd_ensemble_fwd.restype = C.c_int
+    lib.spd_ensemble_fwd_marked.argtypes = lib.spd_ensemble_fwd.argtypes + [C.c_void_p]
+    lib.spd_ensemble_fwd_marked.restype = C.c_int
     lib.spd_vjp_scratch_bytes.argtypes = [P(Desc)]
     lib.spd_vjp_scratch_bytes.restype = C.c_size_t
     lib.spd_vjp.argtypes = [P(Desc), P(VGrid), P(Params), P(Inputs), P(Cotangents), P(Grads),
                             C.c_void_p, C.c_size_t, C.c_void_p]
     lib.spd_vjp.restype = C.c_int
+    lib.spd_preload.argtypes = []
+    lib.spd_preload.restype = C.c_int
+    lib.spd_ensemble_vjp_plan_bytes.argtypes = [P(VjpMember), C.c_int]
+    lib.spd_ensemble_vjp_plan_bytes.restype = C.c_size_t
+    lib.spd_ensemble_vjp_plan.argtypes = [P(Class), C.c_int, P(VjpMember), C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_size_t, P(PlanInfo)]
+    lib.spd_ensemble_vjp_plan.restype = C.c_int
+    lib.spd_ensemble_vjp.argtypes = [P(Class), C.c_int, C.c_void_p, P(PlanInfo), C.c_int,
+                                     C.c_void_p]
+    lib.spd_ensemble_vjp.restype = C.c_int
     for name, spec in EXTRA_DECLS.items():
         fn = getattr(lib, name, None)
         if fn is not None:
@@ -171,3 +190,18 @@ def check(rc, what="spd call"):
     if rc != 0:
         msg = load().spd_status_string(rc).decode()
         raise SpeedyLibraryError(f"{what} failed with status {rc}: {msg}")
+
+
+_preloaded = set()
+
+
+def preload(device_index: int):
+    """Loads every kernel on ``device_index`` once per process (spd_preload), so that lazy
+    module loading never waits on running kernels at a first launch."""
+    if device_index in _preloaded:
+        return
+    import torch
+    lib = load()
+    with torch.cuda.device(device_index):
+        check(lib.spd_preload(), "spd_preload")
+    _preloaded.add(device_index)

@@ -58,6 +58,7 @@ def vjp(physics: SpeedyPhysics, state: PhysicsState, forcing, geometry, date,
     """(PhysicsState of gradients, tensor[12] of parameter gradients) for the cotangent."""
     lib = _lib.load()
     dev = state.temperature.device
+    _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())
     f2 = forcing.day_slice(date.model_day())
     inp, keep = _input_struct(state, f2, geometry)
     ct = {k: getattr(cotangent, k).to(device=dev, dtype=torch.float32).contiguous()

@@ -44,6 +44,7 @@ class Ensemble:
                                   q_tend_scale=q_tend_scale, diagnostics=False)
         dev = members[0].state.temperature.device
         self.device = dev
+        _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())
         keys, classes = {}, []
         cls_of = []
         day = date.model_day()
@@ -105,12 +106,16 @@ class Ensemble:
     def signature(self):
         return tuple(sorted((m.geometry.nodal_shape for m in self.members)))
 
-    def forward(self, grid_blocks=None):
+    def forward(self, grid_blocks=None, marker=None):
+        """Runs every member.  ``marker`` (a torch.cuda.Event) is recorded between the pre-pass
+        and the column pass, for timing the two launches separately."""
         lib = _lib.load()
         gb = self.grid_blocks if grid_blocks is None else grid_blocks
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        rc = lib.spd_ensemble_fwd(self.classes, self.nclasses, C.c_void_p(self.plan.data_ptr()),
-                                  C.byref(self.info), int(gb), C.c_void_p(stream))
+        ev = C.c_void_p(marker.cuda_event) if marker is not None else None
+        rc = lib.spd_ensemble_fwd_marked(self.classes, self.nclasses,
+                                         C.c_void_p(self.plan.data_ptr()), C.byref(self.info),
+                                         int(gb), C.c_void_p(stream), ev)
         _lib.check(rc, "spd_ensemble_fwd")
         return [m.out for m in self.members]
 

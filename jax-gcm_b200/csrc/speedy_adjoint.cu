@@ -1,16 +1,21 @@
-// speedy_adjoint.cu -- the adjoint of the plain forward (spd_vjp).
+// speedy_adjoint.cu -- the adjoint of the forward: one instance (spd_vjp) or a ragged ensemble
+// of them (spd_ensemble_vjp).
 //
 // Launch 1 is the forward's cloud-top pre-pass (the instance level set S and the per-latitude
 // solar table: neither carries a derivative).  Launch 2 runs one thread per column: the
 // hand-written reverse pass of speedy_vjp.h recomputes the column's forward and walks its terms
 // backwards, writing the state gradients.  The 12 parameter gradients are summed per thread,
-// then per block, then with one atomicAdd per block and parameter.
+// then per block, then with one atomicAdd per block and parameter.  The ensemble form runs both
+// launches over the tile list of speedy_ensemble.cuh; its blocks reduce per tile, into the
+// tile's member.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string.h>
+
 #include <algorithm>
 
-#include "speedy_kernels.cuh"
+#include "speedy_ensemble.cuh"
 #include "speedy_vjp.h"
 
 namespace spd {
@@ -20,8 +25,6 @@ Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_
 
 constexpr size_t kAdjHeader = 256;
 constexpr int kAdjBlock = 128;
-
-inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 inline size_t vjp_scratch(const spd_desc_t* d) {
   return kAdjHeader + align256((size_t)d->il * sizeof(ZonalRow));
@@ -35,65 +38,67 @@ struct VjpArgs {
   float ablco2, dt_seconds, q_tend_scale;
 };
 
+// One column's VJP: loads, the reverse pass, stores; adds the parameter gradients to pacc.
+// Not inlined, so that the single-instance and ensemble kernels run the same instructions
+// (inlined, the compiler may contract multiply-adds differently in each caller) and give
+// bitwise-equal gradients.
 template <int KX>
-__global__ void __launch_bounds__(kAdjBlock)
-    adjoint_kernel(const __grid_constant__ VjpArgs A, const spd_inputs_t in,
-                   const spd_cotangents_t ct, const spd_grads_t gr,
-                   const uint32_t* __restrict__ S, const ZonalRow* __restrict__ table) {
-  const int C = A.C;
-  const spdvjp::Ctx x{&A.vg, &A.p, A.flags, A.model_step, __ldg(S)};
+__device__ __noinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t& in,
+                                           const spd_cotangents_t& ct, const spd_grads_t& gr,
+                                           uint32_t Sw, const ZonalRow* __restrict__ table,
+                                           int c, int C, int il, float* pacc) {
+  const spdvjp::Ctx x{&A.vg, &A.p, A.flags, A.model_step, Sw};
   spdgen::DiffParams<float> g;
   g.psmin = A.p.psmin; g.trcnv = A.p.trcnv; g.rhil = A.p.rhil; g.rhbl = A.p.rhbl;
   g.entmax = A.p.entmax; g.smf = A.p.smf; g.trlsc = A.p.trlsc; g.rhlsc = A.p.rhlsc;
   g.drhlsc = A.p.drhlsc; g.rhblsc = A.p.rhblsc; g.albcl = A.p.albcl; g.albcls = A.p.albcls;
-  float pacc[SPD_NUM_DIFF_PARAMS];
-#pragma unroll
-  for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] = 0.0f;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
-    spdgen::ColumnIn<float, float> xi;
-    float ct_t[KX], ct_q[KX];
+  spdgen::ColumnIn<float, float> xi;
+  float ct_t[KX], ct_q[KX];
 #pragma unroll 1
-    for (int k = 0; k < KX; ++k) {
-      const size_t i = (size_t)k * C + c;
-      xi.t[k] = __ldg(in.temperature + i);
-      xi.q[k] = __ldg(in.specific_humidity + i);
-      xi.phi[k] = __ldg(in.geopotential + i);
-      ct_t[k] = __ldg(ct.temperature + i);
-      ct_q[k] = __ldg(ct.specific_humidity + i);
-    }
-    const size_t lo = (size_t)(KX - 1) * C + c;
-    xi.psa = __ldg(in.normalized_surface_pressure + c);
-    xi.u_low = __ldg(in.u_wind + lo);
-    xi.v_low = __ldg(in.v_wind + lo);
-    xi.sst = __ldg(in.sea_surface_temperature + c);
-    xi.stl = __ldg(in.stl_am + c);
-    xi.soilw = __ldg(in.soilw_am + c);
-    xi.snowc = __ldg(in.snowc_am + c);
-    xi.sice = __ldg(in.sice_am + c);
-    xi.alb0 = __ldg(in.alb0 + c);
-    xi.fmask = __ldg(in.fmask + c);
-    xi.orog = __ldg(in.orog + c);
-    xi.phis0 = __ldg(in.phis0 + c);
-    const ZonalRow z = table[c % A.il];
-    xi.fsol = z.fsol; xi.ozupp = z.ozupp; xi.ozone = z.ozone; xi.zenit = z.zenit;
-    xi.stratz = z.stratz; xi.sqrt_coa = z.sqrt_coa;
-    spdvjp::Bar<KX, float> b;
-    spdvjp::column_vjp<KX, float>(x, g, A.ablco2, A.dt_seconds, A.q_tend_scale, xi, ct_t, ct_q,
-                                  __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b);
-#pragma unroll 1
-    for (int k = 0; k < KX; ++k) {
-      const size_t i = (size_t)k * C + c;
-      gr.temperature[i] = b.t[k];
-      gr.specific_humidity[i] = b.q[k];
-      gr.geopotential[i] = b.phi[k];
-      gr.u_wind[i] = (k == KX - 1) ? b.u : 0.0f;
-      gr.v_wind[i] = (k == KX - 1) ? b.v : 0.0f;
-    }
-    gr.normalized_surface_pressure[c] = b.psa;
-#pragma unroll
-    for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] += b.par[j];
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    xi.t[k] = __ldg(in.temperature + i);
+    xi.q[k] = __ldg(in.specific_humidity + i);
+    xi.phi[k] = __ldg(in.geopotential + i);
+    ct_t[k] = __ldg(ct.temperature + i);
+    ct_q[k] = __ldg(ct.specific_humidity + i);
   }
-  // parameter gradients: warp, then block, then one atomic per block and parameter
+  const size_t lo = (size_t)(KX - 1) * C + c;
+  xi.psa = __ldg(in.normalized_surface_pressure + c);
+  xi.u_low = __ldg(in.u_wind + lo);
+  xi.v_low = __ldg(in.v_wind + lo);
+  xi.sst = __ldg(in.sea_surface_temperature + c);
+  xi.stl = __ldg(in.stl_am + c);
+  xi.soilw = __ldg(in.soilw_am + c);
+  xi.snowc = __ldg(in.snowc_am + c);
+  xi.sice = __ldg(in.sice_am + c);
+  xi.alb0 = __ldg(in.alb0 + c);
+  xi.fmask = __ldg(in.fmask + c);
+  xi.orog = __ldg(in.orog + c);
+  xi.phis0 = __ldg(in.phis0 + c);
+  const ZonalRow z = table[c % il];
+  xi.fsol = z.fsol; xi.ozupp = z.ozupp; xi.ozone = z.ozone; xi.zenit = z.zenit;
+  xi.stratz = z.stratz; xi.sqrt_coa = z.sqrt_coa;
+  spdvjp::Bar<KX, float> b;
+  spdvjp::column_vjp<KX, float>(x, g, A.ablco2, A.dt_seconds, A.q_tend_scale, xi, ct_t, ct_q,
+                                __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b);
+#pragma unroll 1
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    gr.temperature[i] = b.t[k];
+    gr.specific_humidity[i] = b.q[k];
+    gr.geopotential[i] = b.phi[k];
+    gr.u_wind[i] = (k == KX - 1) ? b.u : 0.0f;
+    gr.v_wind[i] = (k == KX - 1) ? b.v : 0.0f;
+  }
+  gr.normalized_surface_pressure[c] = b.psa;
+#pragma unroll
+  for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] += b.par[j];
+}
+
+// Sums pacc over the block and adds it to params with one atomic per parameter.  Every thread
+// of the block must call it.
+__device__ __forceinline__ void block_add_params(float* pacc, float* params) {
   __shared__ float red[kAdjBlock / 32][SPD_NUM_DIFF_PARAMS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -106,7 +111,73 @@ __global__ void __launch_bounds__(kAdjBlock)
   if (threadIdx.x < SPD_NUM_DIFF_PARAMS) {
     float v = 0.0f;
     for (int w = 0; w < kAdjBlock / 32; ++w) v += red[w][threadIdx.x];
-    atomicAdd(gr.params + threadIdx.x, v);
+    atomicAdd(params + threadIdx.x, v);
+  }
+  __syncthreads();
+}
+
+template <int KX>
+__global__ void __launch_bounds__(kAdjBlock, 3)
+    adjoint_kernel(const __grid_constant__ VjpArgs A, const spd_inputs_t in,
+                   const spd_cotangents_t ct, const spd_grads_t gr,
+                   const uint32_t* __restrict__ S, const ZonalRow* __restrict__ table) {
+  const uint32_t Sw = __ldg(S);
+  float pacc[SPD_NUM_DIFF_PARAMS];
+#pragma unroll
+  for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] = 0.0f;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.C; c += gridDim.x * blockDim.x)
+    vjp_column<KX>(A, in, ct, gr, Sw, table, c, A.C, A.il, pacc);
+  block_add_params(pacc, gr.params);
+}
+
+// ---- ensemble ----
+struct VjpMemberDev {
+  spd_inputs_t in;
+  spd_cotangents_t ct;
+  spd_grads_t gr;
+  int C, il, kx, cls;
+  uint32_t* S;
+  ZonalRow* table;
+};
+
+struct VjpClassArgs {
+  VjpArgs cls[SPD_MAX_CLASSES];
+};
+
+__global__ void __launch_bounds__(kBlock)
+    ensemble_vjp_prepass(const __grid_constant__ ClassArgs A,
+                         const VjpMemberDev* __restrict__ members,
+                         const Tile* __restrict__ tiles, int ntiles) {
+  // the adjoint launch accumulates each member's parameter gradients: zero them here
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    if (tl.col0 == 0 && threadIdx.x < SPD_NUM_DIFF_PARAMS)
+      members[tl.member].gr.params[threadIdx.x] = 0.0f;
+  }
+  prepass_tiles(A, members, tiles, ntiles);
+}
+
+__global__ void __launch_bounds__(kAdjBlock, 3)
+    ensemble_adjoint(const __grid_constant__ VjpClassArgs A,
+                     const VjpMemberDev* __restrict__ members, const Tile* __restrict__ tiles,
+                     int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const VjpMemberDev& m = members[tl.member];
+    const int c = tl.col0 + threadIdx.x;
+    float pacc[SPD_NUM_DIFF_PARAMS];
+#pragma unroll
+    for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] = 0.0f;
+    if (c < m.C) {
+      const VjpArgs& V = A.cls[m.cls];
+      const uint32_t Sw = *m.S;
+      switch (m.kx) {  // uniform per block
+        case 16: vjp_column<16>(V, m.in, m.ct, m.gr, Sw, m.table, c, m.C, m.il, pacc); break;
+        case 8: vjp_column<8>(V, m.in, m.ct, m.gr, Sw, m.table, c, m.C, m.il, pacc); break;
+        default: vjp_column<7>(V, m.in, m.ct, m.gr, Sw, m.table, c, m.C, m.il, pacc); break;
+      }
+    }
+    block_add_params(pacc, m.gr.params);
   }
 }
 
@@ -123,6 +194,54 @@ static int launch_vjp(const VjpArgs& A, const Consts& K, const spd_inputs_t& in,
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
+int preload_adjoint() {
+  cudaFuncAttributes a;
+  bool ok = true;
+  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<7>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<8>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<16>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<7>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<8>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<16>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_vjp_prepass) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_adjoint) == cudaSuccess;
+  return ok ? SPD_OK : SPD_ERR_CUDA;
+}
+
+static VjpArgs make_vjp_args(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
+                             const spd_params_t* params) {
+  const Derived D = derive_constants(desc, vgrid, params);
+  VjpArgs A;
+  A.vg = *vgrid;
+  A.p = *params;
+  A.flags = desc->flags;
+  A.model_step = desc->model_step;
+  A.C = desc->ix * desc->il;
+  A.il = desc->il;
+  A.ablco2 = D.ablco2;
+  A.dt_seconds = desc->dt_seconds;
+  A.q_tend_scale = desc->q_tend_scale;
+  return A;
+}
+
+// The fields spd_vjp reads and writes, validated like spd_fwd's.
+static int check_vjp_member(const spd_desc_t* desc, const spd_inputs_t* in,
+                            const spd_cotangents_t* ct, const spd_grads_t* grads) {
+  if (!desc || !in || !ct || !grads) return SPD_ERR_NULL;
+  spd_outputs_t dummy = {};
+  float* probe = grads->temperature;
+  dummy.u_wind = dummy.v_wind = dummy.temperature = dummy.specific_humidity = probe;
+  dummy.precnv = dummy.precls = probe;
+  int rc = check_instance(desc, in, &dummy);
+  if (rc != SPD_OK) return rc;
+  const void* req[] = {ct->u_wind, ct->v_wind, ct->temperature, ct->specific_humidity,
+                       grads->u_wind, grads->v_wind, grads->specific_humidity,
+                       grads->geopotential, grads->normalized_surface_pressure, grads->params};
+  for (const void* p : req)
+    if (!p) return SPD_ERR_NULL;
+  return SPD_OK;
+}
+
 }  // namespace spd
 
 extern "C" {
@@ -137,33 +256,14 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
             void* scratch, size_t scratch_bytes, void* stream) {
   using namespace spd;
   if (!desc || !vgrid || !params || !in || !ct || !grads) return SPD_ERR_NULL;
-  spd_outputs_t dummy = {};
-  float* probe = grads->temperature;
-  dummy.u_wind = dummy.v_wind = dummy.temperature = dummy.specific_humidity = probe;
-  dummy.precnv = dummy.precls = probe;
-  int rc = check_instance(desc, in, &dummy);
+  const int rc = check_vjp_member(desc, in, ct, grads);
   if (rc != SPD_OK) return rc;
-  const void* req[] = {ct->u_wind, ct->v_wind, ct->temperature, ct->specific_humidity,
-                       grads->u_wind, grads->v_wind, grads->specific_humidity,
-                       grads->geopotential, grads->normalized_surface_pressure, grads->params};
-  for (const void* p : req)
-    if (!p) return SPD_ERR_NULL;
   if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) ||
       scratch_bytes < vjp_scratch(desc))
     return SPD_ERR_SCRATCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const Consts K = make_consts(desc, vgrid, params);
-  const Derived D = derive_constants(desc, vgrid, params);
-  VjpArgs A;
-  A.vg = *vgrid;
-  A.p = *params;
-  A.flags = desc->flags;
-  A.model_step = desc->model_step;
-  A.C = desc->ix * desc->il;
-  A.il = desc->il;
-  A.ablco2 = D.ablco2;
-  A.dt_seconds = desc->dt_seconds;
-  A.q_tend_scale = desc->q_tend_scale;
+  const VjpArgs A = make_vjp_args(desc, vgrid, params);
   char* sc = static_cast<char*>(scratch);
   if (cudaMemsetAsync(sc, 0, kAdjHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
   if (cudaMemsetAsync(grads->params, 0, SPD_NUM_DIFF_PARAMS * sizeof(float), st) != cudaSuccess)
@@ -174,6 +274,81 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
     case 16: return launch_vjp<16>(A, K, *in, *ct, *grads, sc, st);
     default: return SPD_ERR_KX;
   }
+}
+
+size_t spd_ensemble_vjp_plan_bytes(const spd_vjp_member_t* members, int nmembers) {
+  if (!members || nmembers <= 0) return 0;
+  return spd::plan_layout(members, nmembers, sizeof(spd::VjpMemberDev)).total;
+}
+
+int spd_ensemble_vjp_plan(const spd_class_t* classes, int nclasses,
+                          const spd_vjp_member_t* members, int nmembers, void* plan_host,
+                          void* plan_device, size_t plan_bytes, spd_plan_info_t* info) {
+  using namespace spd;
+  if (!classes || !members || !plan_host || !plan_device || !info) return SPD_ERR_NULL;
+  if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || nmembers <= 0) return SPD_ERR_SHAPE;
+  if (reinterpret_cast<uintptr_t>(plan_device) & 255u) return SPD_ERR_SCRATCH;
+  const PlanLayout L = plan_layout(members, nmembers, sizeof(VjpMemberDev));
+  if (plan_bytes < L.total) return SPD_ERR_SCRATCH;
+  for (int i = 0; i < nmembers; ++i) {
+    const spd_vjp_member_t& m = members[i];
+    if (m.cls < 0 || m.cls >= nclasses) return SPD_ERR_SHAPE;
+    spd_desc_t d = classes[m.cls].desc;
+    d.ix = m.ix;
+    d.il = m.il;
+    const int rc = check_vjp_member(&d, &m.in, &m.ct, &m.grads);
+    if (rc != SPD_OK) return rc;
+  }
+  char* h = static_cast<char*>(plan_host);
+  memset(h, 0, L.total);
+  VjpMemberDev* md = reinterpret_cast<VjpMemberDev*>(h + L.members);
+  for (int i = 0; i < nmembers; ++i) {
+    const spd_vjp_member_t& m = members[i];
+    md[i].in = m.in;
+    md[i].ct = m.ct;
+    md[i].gr = m.grads;
+    md[i].C = m.ix * m.il;
+    md[i].il = m.il;
+    md[i].kx = classes[m.cls].desc.kx;
+    md[i].cls = m.cls;
+  }
+  const int t = plan_tiles(md, nmembers, L, static_cast<char*>(plan_device),
+                           reinterpret_cast<Tile*>(h + L.tiles));
+  info->nmembers = nmembers;
+  info->ntiles = t;
+  info->levelset_offset = L.levelset;
+  info->levelset_bytes = align256((size_t)nmembers * sizeof(uint32_t));
+  info->plan_bytes = L.total;
+  return SPD_OK;
+}
+
+int spd_ensemble_vjp(const spd_class_t* classes, int nclasses, void* plan_device,
+                     const spd_plan_info_t* info, int grid_blocks, void* stream) {
+  using namespace spd;
+  if (!classes || !plan_device || !info) return SPD_ERR_NULL;
+  if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
+  ClassArgs P;
+  VjpClassArgs V;
+  for (int i = 0; i < nclasses; ++i) {
+    P.cls[i].K = make_consts(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+    P.cls[i].D = derive_constants(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+    V.cls[i] = make_vjp_args(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+  }
+  // Default: one block per tile.  The blocks are short (one tile's columns each), so the SMs
+  // turn over often and a higher-priority stream's kernels (a forward batch) get them within
+  // one block's time; a persistent grid would hold every SM until the whole batch is done.
+  int grid = grid_blocks > 0 ? std::min(grid_blocks, info->ntiles) : info->ntiles;
+  const int grid_pre = std::min(info->ntiles, 65535);
+  char* base = static_cast<char*>(plan_device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const VjpMemberDev* md = reinterpret_cast<const VjpMemberDev*>(base + 256);
+  const size_t tiles_off = 256 + align256((size_t)info->nmembers * sizeof(VjpMemberDev));
+  const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
+  if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
+    return SPD_ERR_CUDA;
+  ensemble_vjp_prepass<<<grid_pre, kBlock, 0, st>>>(P, md, tl, info->ntiles);
+  ensemble_adjoint<<<grid, kAdjBlock, 0, st>>>(V, md, tl, info->ntiles);
+  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
 }  // extern "C"

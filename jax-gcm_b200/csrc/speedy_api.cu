@@ -63,7 +63,7 @@ Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_
 
 template <int KX>
 static int launch_fwd(const ConstsD& CD, const spd_inputs_t& in, const spd_outputs_t& out,
-                      uint32_t* S, ZonalRow* table, cudaStream_t st) {
+                      uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker) {
   static bool attr_done = false;  // per template instance; idempotent, so races are harmless
   if (!attr_done) {
     if (cudaFuncSetAttribute(column_kernel<KX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -75,23 +75,48 @@ static int launch_fwd(const ConstsD& CD, const spd_inputs_t& in, const spd_outpu
   const int grid = (K.C + kNT - 1) / kNT;
   const int grid_a = (max(K.C, K.il) + kBlock - 1) / kBlock;
   cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
+  if (marker && cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
   column_kernel<KX><<<grid, kNT, smem_bytes<KX>(), st>>>(CD, in, out, S, table);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
-                 uint32_t* S, ZonalRow* table, cudaStream_t st) {
+                 uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker) {
   switch (kx) {
-    case 7: return launch_fwd<7>(CD, in, out, S, table, st);
-    case 8: return launch_fwd<8>(CD, in, out, S, table, st);
-    case 16: return launch_fwd<16>(CD, in, out, S, table, st);
+    case 7: return launch_fwd<7>(CD, in, out, S, table, st, marker);
+    case 8: return launch_fwd<8>(CD, in, out, S, table, st, marker);
+    case 16: return launch_fwd<16>(CD, in, out, S, table, st, marker);
     default: return SPD_ERR_KX;
   }
+}
+
+int preload_ensemble();
+int preload_adjoint();
+
+// Loads this translation unit's kernels (see spd_preload).
+static int preload_api() {
+  cudaFuncAttributes a;
+  bool ok = true;
+  ok &= cudaFuncGetAttributes(&a, column_kernel<7>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, column_kernel<8>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, column_kernel<16>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<7>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<8>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<16>) == cudaSuccess;
+  return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 
 }  // namespace spd
 
 extern "C" {
+
+int spd_preload(void) {
+  const int a = spd::preload_api();
+  const int b = spd::preload_ensemble();
+  const int c = spd::preload_adjoint();
+  return (a == SPD_OK && b == SPD_OK && c == SPD_OK) ? SPD_OK : SPD_ERR_CUDA;
+}
+
 
 size_t spd_fwd_scratch_bytes(const spd_desc_t* desc) {
   if (!desc || desc->il <= 0) return 0;
@@ -102,6 +127,12 @@ size_t spd_fwd_scratch_bytes(const spd_desc_t* desc) {
 int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
             const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
             size_t scratch_bytes, void* stream) {
+  return spd_fwd_marked(desc, vgrid, params, in, out, scratch, scratch_bytes, stream, nullptr);
+}
+
+int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
+                   const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
+                   size_t scratch_bytes, void* stream, void* event) {
   int rc = spd::check_instance(desc, in, out);
   if (rc != SPD_OK) return rc;
   if (!vgrid || !params) return SPD_ERR_NULL;
@@ -116,7 +147,8 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
   spd::ZonalRow* table =
       reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + spd::kHeaderBytes);
   if (cudaMemsetAsync(S, 0, spd::kHeaderBytes, st) != cudaSuccess) return SPD_ERR_CUDA;
-  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st);
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st,
+                           static_cast<cudaEvent_t>(event));
 }
 
 const char* spd_status_string(int status) {

@@ -17,53 +17,18 @@
 #include <algorithm>
 #include <vector>
 
-#include "speedy_kernels.cuh"
+#include "speedy_ensemble.cuh"
 
 namespace spd {
 
 int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
-struct MemberDev {
-  spd_inputs_t in;
-  spd_outputs_t out;
-  int C, il, kx, cls;
-  uint32_t* S;
-  ZonalRow* table;
-};
-
-struct ClassArgs {
-  ConstsD cls[SPD_MAX_CLASSES];
-};
-
-struct Tile {
-  int member, col0;
-};
-
-constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-
-template <int KX>
-__device__ __forceinline__ void prepass_tile(const ClassArgs& A, const MemberDev& m, int c) {
-  const Consts& K = A.cls[m.cls].K;
-  if (c < m.il) m.table[c] = zonal_row(K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
-  const uint32_t bit = (c < m.C) ? prepass_column<KX>(K, m.in, c, m.C) : 0u;
-  or_level_set(bit, m.S);
-}
-
 __global__ void __launch_bounds__(kBlock) ensemble_prepass(const __grid_constant__ ClassArgs A,
                                                            const MemberDev* __restrict__ members,
                                                            const Tile* __restrict__ tiles,
                                                            int ntiles) {
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    const MemberDev& m = members[tl.member];
-    const int c = tl.col0 + threadIdx.x;
-    switch (m.kx) {  // uniform per block
-      case 16: prepass_tile<16>(A, m, c); break;
-      case 8: prepass_tile<8>(A, m, c); break;
-      default: prepass_tile<7>(A, m, c); break;
-    }
-  }
+  prepass_tiles(A, members, tiles, ntiles);
 }
 
 __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant__ ClassArgs A,
@@ -87,27 +52,11 @@ __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant
   }
 }
 
-struct Layout {
-  size_t members, tiles, levelset, tables, total;
-  int ntiles;
-};
-
-static Layout layout_of(const spd_member_t* members, int n) {
-  Layout L;
-  int ntiles = 0;
-  size_t tab = 0;
-  for (int i = 0; i < n; ++i) {
-    const int C = members[i].ix * members[i].il;
-    ntiles += (C + kNT - 1) / kNT;
-    tab += align256((size_t)members[i].il * sizeof(ZonalRow));
-  }
-  L.ntiles = ntiles;
-  L.members = 256;
-  L.tiles = L.members + align256((size_t)n * sizeof(MemberDev));
-  L.levelset = L.tiles + align256((size_t)ntiles * sizeof(Tile));
-  L.tables = L.levelset + align256((size_t)n * sizeof(uint32_t));
-  L.total = L.tables + tab;
-  return L;
+int preload_ensemble() {
+  cudaFuncAttributes a;
+  bool ok = cudaFuncGetAttributes(&a, ensemble_prepass) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_columns) == cudaSuccess;
+  return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 
 }  // namespace spd
@@ -116,7 +65,7 @@ extern "C" {
 
 size_t spd_ensemble_plan_bytes(const spd_member_t* members, int nmembers) {
   if (!members || nmembers <= 0) return 0;
-  return spd::layout_of(members, nmembers).total;
+  return spd::plan_layout(members, nmembers, sizeof(spd::MemberDev)).total;
 }
 
 int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member_t* members,
@@ -126,7 +75,7 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
   if (!classes || !members || !plan_host || !plan_device || !info) return SPD_ERR_NULL;
   if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || nmembers <= 0) return SPD_ERR_SHAPE;
   if (reinterpret_cast<uintptr_t>(plan_device) & 255u) return SPD_ERR_SCRATCH;
-  const Layout L = layout_of(members, nmembers);
+  const PlanLayout L = plan_layout(members, nmembers, sizeof(MemberDev));
   if (plan_bytes < L.total) return SPD_ERR_SCRATCH;
   for (int i = 0; i < nmembers; ++i) {
     const spd_member_t& m = members[i];
@@ -141,7 +90,6 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
   char* dbase = static_cast<char*>(plan_device);
   memset(h, 0, L.total);
   MemberDev* md = reinterpret_cast<MemberDev*>(h + L.members);
-  size_t tab = L.tables;
   for (int i = 0; i < nmembers; ++i) {
     const spd_member_t& m = members[i];
     md[i].in = m.in;
@@ -150,19 +98,8 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
     md[i].il = m.il;
     md[i].kx = classes[m.cls].desc.kx;
     md[i].cls = m.cls;
-    md[i].S = reinterpret_cast<uint32_t*>(dbase + L.levelset) + i;
-    md[i].table = reinterpret_cast<ZonalRow*>(dbase + tab);
-    tab += align256((size_t)m.il * sizeof(ZonalRow));
   }
-  // tiles: 16-level members first, then fewer levels (heavier work first)
-  std::vector<int> order(nmembers);
-  for (int i = 0; i < nmembers; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return md[a].kx > md[b].kx; });
-  Tile* tl = reinterpret_cast<Tile*>(h + L.tiles);
-  int t = 0;
-  for (int i : order)
-    for (int c0 = 0; c0 < md[i].C; c0 += kNT) tl[t++] = Tile{i, c0};
+  const int t = plan_tiles(md, nmembers, L, dbase, reinterpret_cast<Tile*>(h + L.tiles));
   info->nmembers = nmembers;
   info->ntiles = t;
   info->levelset_offset = L.levelset;
@@ -173,6 +110,13 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
 
 int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device,
                      const spd_plan_info_t* info, int grid_blocks, void* stream) {
+  return spd_ensemble_fwd_marked(classes, nclasses, plan_device, info, grid_blocks, stream,
+                                 nullptr);
+}
+
+int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
+                            const spd_plan_info_t* info, int grid_blocks, void* stream,
+                            void* event) {
   using namespace spd;
   if (!classes || !plan_device || !info) return SPD_ERR_NULL;
   if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
@@ -207,6 +151,8 @@ int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device
   if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
     return SPD_ERR_CUDA;
   ensemble_prepass<<<grid * 2, kBlock, 0, st>>>(A, md, tl, info->ntiles);
+  if (event && cudaEventRecord(static_cast<cudaEvent_t>(event), st) != cudaSuccess)
+    return SPD_ERR_CUDA;
   ensemble_columns<<<grid, kNT, smem_bytes<16>(), st>>>(A, md, tl, info->ntiles);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }

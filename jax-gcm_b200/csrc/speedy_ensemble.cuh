@@ -1,0 +1,101 @@
+// speedy_ensemble.cuh -- what the batched forward and the batched adjoint share: the tile
+// list over ragged members, the per-class constants passed by value, and the cloud-top
+// pre-pass over all tiles (each member's level set and per-latitude solar table).
+#pragma once
+
+#include <algorithm>
+#include <vector>
+
+#include "speedy_kernels.cuh"
+
+namespace spd {
+
+struct MemberDev {
+  spd_inputs_t in;
+  spd_outputs_t out;
+  int C, il, kx, cls;
+  uint32_t* S;
+  ZonalRow* table;
+};
+
+struct ClassArgs {
+  ConstsD cls[SPD_MAX_CLASSES];
+};
+
+struct Tile {
+  int member, col0;
+};
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// M: any member record with in, C, il, kx, cls, S and table.
+template <int KX, class M>
+__device__ __forceinline__ void prepass_tile(const ClassArgs& A, const M& m, int c) {
+  const Consts& K = A.cls[m.cls].K;
+  if (c < m.il) m.table[c] = zonal_row(K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
+  const uint32_t bit = (c < m.C) ? prepass_column<KX>(K, m.in, c, m.C) : 0u;
+  or_level_set(bit, m.S);
+}
+
+template <class M>
+__device__ __forceinline__ void prepass_tiles(const ClassArgs& A, const M* __restrict__ members,
+                                              const Tile* __restrict__ tiles, int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const M& m = members[tl.member];
+    const int c = tl.col0 + threadIdx.x;
+    switch (m.kx) {  // uniform per block
+      case 16: prepass_tile<16>(A, m, c); break;
+      case 8: prepass_tile<8>(A, m, c); break;
+      default: prepass_tile<7>(A, m, c); break;
+    }
+  }
+}
+
+// Device plan layout: header, member records, tile list, level-set words, solar tables.
+struct PlanLayout {
+  size_t members, tiles, levelset, tables, total;
+  int ntiles;
+};
+
+// HM: host member description with ix and il.
+template <class HM>
+inline PlanLayout plan_layout(const HM* members, int n, size_t record_bytes) {
+  PlanLayout L;
+  int ntiles = 0;
+  size_t tab = 0;
+  for (int i = 0; i < n; ++i) {
+    const int C = members[i].ix * members[i].il;
+    ntiles += (C + kNT - 1) / kNT;
+    tab += align256((size_t)members[i].il * sizeof(ZonalRow));
+  }
+  L.ntiles = ntiles;
+  L.members = 256;
+  L.tiles = L.members + align256((size_t)n * record_bytes);
+  L.levelset = L.tiles + align256((size_t)ntiles * sizeof(Tile));
+  L.tables = L.levelset + align256((size_t)n * sizeof(uint32_t));
+  L.total = L.tables + tab;
+  return L;
+}
+
+// Fills each record's level-set and table pointers (device addresses) and the tile list:
+// tiles of 16-level members first, then fewer levels (heavier work first).  Returns the tile
+// count.  DM: device member record with C, il, kx, S and table.
+template <class DM>
+inline int plan_tiles(DM* md, int n, const PlanLayout& L, char* dbase, Tile* tl) {
+  size_t tab = L.tables;
+  for (int i = 0; i < n; ++i) {
+    md[i].S = reinterpret_cast<uint32_t*>(dbase + L.levelset) + i;
+    md[i].table = reinterpret_cast<ZonalRow*>(dbase + tab);
+    tab += align256((size_t)md[i].il * sizeof(ZonalRow));
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return md[a].kx > md[b].kx; });
+  int t = 0;
+  for (int i : order)
+    for (int c0 = 0; c0 < md[i].C; c0 += kNT) tl[t++] = Tile{i, c0};
+  return t;
+}
+
+}  // namespace spd

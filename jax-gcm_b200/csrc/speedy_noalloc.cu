@@ -19,7 +19,7 @@ namespace spd {
 int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
-                 uint32_t* S, ZonalRow* table, cudaStream_t st);
+                 uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker);
 }  // namespace spd
 
 namespace {
@@ -71,5 +71,5 @@ extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
   // The array keeps the previous call's contents: the level-set and status words must start
   // at zero; the solar table is fully rewritten by the pre-pass.
   if (cudaMemsetAsync(S, 0, kNoallocHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
-  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st);
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st, nullptr);
 }

@@ -462,7 +462,10 @@ class SpeedyPhysics(Physics):
         return buf
 
     def compute_tendencies(self, state: PhysicsState, forcing: ForcingData, geometry: Geometry,
-                           date: DateData, out: Optional[dict] = None):
+                           date: DateData, out: Optional[dict] = None, marker=None):
+        """Tendencies and PhysicsData for ``state``.  ``out`` may give preallocated output
+        tensors; ``marker`` (a torch.cuda.Event) is recorded between the cloud-top pre-pass and
+        the column kernel, for timing the two launches separately."""
         lib = _lib.load()
         kx, ix, il = geometry.nodal_shape
         t = state.temperature
@@ -471,6 +474,7 @@ class SpeedyPhysics(Physics):
         dev = t.device
         if dev.type != "cuda":
             raise RuntimeError("SpeedyPhysics runs on CUDA tensors only (no CPU path)")
+        _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())
         f2 = forcing.day_slice(date.model_day())
         tensors = dict(u_wind=state.u_wind, v_wind=state.v_wind, temperature=state.temperature,
                        specific_humidity=state.specific_humidity,
@@ -500,9 +504,10 @@ class SpeedyPhysics(Physics):
         desc = self.desc(geometry, date, forcing.lfluxland)
         scratch = self._scratch_for(desc, dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        rc = lib.spd_fwd(C.byref(desc), C.byref(geometry.vgrid()), C.byref(self._pstruct),
-                         C.byref(inp), C.byref(outs), _ptr(scratch), scratch.numel(),
-                         C.c_void_p(stream))
+        ev = C.c_void_p(marker.cuda_event) if marker is not None else None
+        rc = lib.spd_fwd_marked(C.byref(desc), C.byref(geometry.vgrid()), C.byref(self._pstruct),
+                                C.byref(inp), C.byref(outs), _ptr(scratch), scratch.numel(),
+                                C.c_void_p(stream), ev)
         _lib.check(rc, "spd_fwd")
         tend = PhysicsTendency(out["u_wind"], out["v_wind"], out["temperature"],
                                out["specific_humidity"])

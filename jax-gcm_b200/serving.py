@@ -14,16 +14,19 @@ layer a forecast service would put in front of the physics:
 * Device-resident column state.  A member's state, forcing and geometry are uploaded once, as
   one packed buffer from pinned host memory on a copy stream, and stay on the device while any
   request uses them (and afterwards, until evicted).
-* Continuous batching.  Tendency requests admitted while earlier batches run are merged into
-  the next batch: one ragged-ensemble launch pair (``spd_ensemble_fwd``) over all their members,
-  enqueued while up to ``max_inflight`` earlier batches are still on the device.  VJP requests
-  run on their own stream (``spd_vjp`` per member), so their work overlaps the tendency batches
-  on the device, and uploads overlap both.
+* Continuous batching.  Requests admitted while earlier batches run are merged into the next
+  batch of their kind: one ragged-ensemble launch pair over all their members
+  (``spd_ensemble_fwd`` for tendencies, ``spd_ensemble_vjp`` for VJPs), enqueued while up to
+  ``max_inflight`` earlier batches of that kind are still on the device.  VJP batches run on
+  their own stream, so their work overlaps the tendency batches on the device, and uploads
+  overlap both; the tendency stream has the higher priority.
 * Latency.  Completion times are device timestamps (CUDA events) mapped onto the host clock on
   which arrivals are stamped; p50/p99 latency and columns/s are reported per run.
 
 ``mode="plain"`` is the per-request drop-in on the same GPU: one request at a time in arrival
-order, every member through ``spd_fwd`` (or ``spd_vjp``) on one stream.
+order, every member through ``spd_fwd`` (or ``spd_vjp``) on one stream.  A VJP request's
+cotangents are N(0, 1) drawn once over its contiguous cotangent buffer from a generator seeded
+by the request, in either mode.
 
 The scheduler (``Scheduler``) is independent of the device; ``CudaBackend`` performs the device
 work through the C ABI.  Failures a caller can cause are handled on the host: malformed
@@ -133,6 +136,10 @@ class Request:
     _shapes: list = field(default_factory=list, repr=False)
     _outputs: object = field(default=None, repr=False)
     _out_bytes: int = 0
+    _out_handle: object = field(default=None, repr=False)
+    _views: object = field(default=None, repr=False)
+    _ct: object = field(default=None, repr=False)
+    _base: int = 0
 
     @property
     def latency(self):
@@ -169,7 +176,8 @@ class Scheduler:
 
     def __init__(self, backend, source: Callable[[Hashable], HostMember], budget_bytes: int,
                  mode: str = "batched", max_inflight: int = 2, max_batch_columns: int = 1 << 24,
-                 on_complete: Optional[Callable[[Request], None]] = None):
+                 on_complete: Optional[Callable[[Request], None]] = None,
+                 max_admit_per_step: int = 8):
         if mode not in ("batched", "plain"):
             raise ValueError("mode is 'batched' or 'plain'")
         self.b = backend
@@ -179,6 +187,7 @@ class Scheduler:
         self.max_inflight = max_inflight
         self.max_batch_columns = max_batch_columns
         self.on_complete = on_complete
+        self.max_admit_per_step = max_admit_per_step
         self.used = self.b.fixed_bytes()
         if self.used > self.budget:
             raise ValueError(f"budget {self.budget} below the fixed device bytes {self.used}")
@@ -314,10 +323,32 @@ class Scheduler:
                 r.refs -= 1
 
     def admit(self):
+        """Admits waiting requests in arrival order while they fit, at most
+        ``max_admit_per_step`` per call so that launches interleave with a large burst."""
         n = 0
-        while self.waiting and self._admit_one(self.waiting[0]):
+        while (self.waiting and n < self.max_admit_per_step and
+               self._admit_one(self.waiting[0])):
             self.waiting.popleft()
             n += 1
+        return n
+
+    def prefetch(self, keys):
+        """Makes the members ``keys`` resident ahead of traffic (as far as the budget allows,
+        evicting idle members least-recently-used) and waits for the uploads.  Returns the
+        number uploaded."""
+        n = 0
+        for k in dict.fromkeys(keys):
+            if k in self.resident:
+                continue
+            h = self._host(k)
+            if not self._evict_for(self.b.member_bytes(h), {k}):
+                break
+            self.resident[k] = _Resident(k, h, self.b.upload(h))
+            self.used += self.b.member_bytes(h)
+            self.peak = max(self.peak, self.used)
+            self.stats["prefetched"] += 1
+            n += 1
+        self.b.synchronize()
         return n
 
     # -- launching ------------------------------------------------------------------------------
@@ -346,19 +377,18 @@ class Scheduler:
                 self._launch(r.kind, [r])
                 n += 1
             return n
-        q = self.admitted[TENDENCY]
-        while q and self._inflight_of(TENDENCY) < self.max_inflight:
-            batch, cols = [], 0
-            while q and (not batch or cols + q[0].columns <= self.max_batch_columns):
-                r = q.popleft()
-                batch.append(r)
-                cols += r.columns
-            self._launch(TENDENCY, batch)
-            n += 1
-        q = self.admitted[VJP]
-        while q and self._inflight_of(VJP) < self.max_inflight:
-            self._launch(VJP, [q.popleft()])
-            n += 1
+        # continuous batching: everything admitted of one kind (up to max_batch_columns)
+        # becomes one batched launch while fewer than max_inflight of that kind are on the GPU
+        for kind in KINDS:
+            q = self.admitted[kind]
+            while q and self._inflight_of(kind) < self.max_inflight:
+                batch, cols = [], 0
+                while q and (not batch or cols + q[0].columns <= self.max_batch_columns):
+                    r = q.popleft()
+                    batch.append(r)
+                    cols += r.columns
+                self._launch(kind, batch)
+                n += 1
         return n
 
     # -- completion -----------------------------------------------------------------------------
@@ -496,10 +526,104 @@ def synthetic_source(base_seed=5000, pin=True):
 
 
 # ---------------------------------------------------------------------------------------------
+# Device arena
+# ---------------------------------------------------------------------------------------------
+class DeviceArena:
+    """Best-fit allocator over a few large device chunks, so that serving never calls into the
+    driver's allocator on the request path (a cudaMalloc of a fresh segment takes milliseconds).
+
+    The scheduler frees a buffer only after every kernel that used it has completed (member
+    state when no admitted request references it, results after the completion event), so a
+    freed range can be handed out again at once, on any stream.  Chunks are added on demand
+    (``chunk_bytes`` or the request, whichever is larger) and kept."""
+
+    ALIGN = 256
+
+    def __init__(self, device, chunk_bytes=8 << 30, alloc=None):
+        import torch
+        self.torch = torch
+        self.device = device
+        self.chunk_bytes = int(chunk_bytes)
+        self._alloc = alloc or (lambda n: torch.empty(n, dtype=torch.uint8, device=device))
+        self.chunks = []          # uint8 tensors
+        self.free = []            # per chunk: sorted list of [offset, size]
+        self.reserved = 0
+        self.in_use = 0
+
+    def reserve(self, nbytes):
+        """Adds a chunk of at least nbytes."""
+        n = self.chunk_bytes if nbytes <= self.chunk_bytes else _round_up(int(nbytes), 2 << 20)
+        t = self._alloc(n)
+        self.chunks.append(t)
+        self.free.append([[0, n]])
+        self.reserved += n
+        return len(self.chunks) - 1
+
+    def alloc(self, nbytes):
+        """A uint8 device tensor of nbytes (256-byte aligned), and its handle for release()."""
+        n = _round_up(max(int(nbytes), 1), self.ALIGN)
+        best = None
+        for ci, fl in enumerate(self.free):
+            for j, (off, size) in enumerate(fl):
+                if size >= n and (best is None or size < best[3]):
+                    best = (ci, j, off, size)
+        if best is None:
+            ci = self.reserve(n)
+            best = (ci, 0, 0, self.free[ci][0][1])
+        ci, j, off, size = best
+        if size == n:
+            del self.free[ci][j]
+        else:
+            self.free[ci][j] = [off + n, size - n]
+        self.in_use += n
+        return self.chunks[ci][off:off + n], (ci, off, n)
+
+    def release(self, handle):
+        ci, off, n = handle
+        fl = self.free[ci]
+        lo, hi = 0, len(fl)
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if fl[mid][0] < off:
+                lo = mid + 1
+            else:
+                hi = mid
+        fl.insert(lo, [off, n])
+        # coalesce with the neighbours
+        if lo + 1 < len(fl) and fl[lo][0] + fl[lo][1] == fl[lo + 1][0]:
+            fl[lo][1] += fl[lo + 1][1]
+            del fl[lo + 1]
+        if lo > 0 and fl[lo - 1][0] + fl[lo - 1][1] == fl[lo][0]:
+            fl[lo - 1][1] += fl[lo][1]
+            del fl[lo]
+        self.in_use -= n
+
+
+class PinnedCache:
+    """Reusable pinned host buffers for plans (a pinned allocation costs milliseconds)."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.pool = []
+
+    def get(self, nbytes):
+        for i, t in enumerate(self.pool):
+            if t.numel() >= nbytes:
+                return self.pool.pop(i)
+        return self.torch.empty(max(int(nbytes), 1 << 20) * 2, dtype=self.torch.uint8,
+                                pin_memory=True)
+
+    def put(self, t):
+        self.pool.append(t)
+        self.pool.sort(key=lambda x: x.numel())
+
+
+# ---------------------------------------------------------------------------------------------
 # CUDA backend
 # ---------------------------------------------------------------------------------------------
 class _DevMember:
-    __slots__ = ("host", "buf", "inputs", "ready")
+    __slots__ = ("host", "buf", "inputs", "ready", "handle")
 
     def __init__(self, host, buf, inputs, ready):
         self.host, self.buf, self.inputs, self.ready = host, buf, inputs, ready
@@ -515,7 +639,8 @@ class _Handle:
 class CudaBackend:
     """Device work of the serving loop through the C ABI (ensemble, plain and VJP calls)."""
 
-    def __init__(self, device="cuda", date=None, parameters=None, mode="batched"):
+    def __init__(self, device="cuda", date=None, parameters=None, mode="batched",
+                 arena_chunk_bytes=8 << 30, reserve_bytes=0):
         import torch
         from .physics import DateData, SpeedyPhysics, initialize_vertical
         self.torch = torch
@@ -523,10 +648,13 @@ class CudaBackend:
         self.dev = torch.device(device)
         if self.dev.index is None:
             self.dev = torch.device("cuda", torch.cuda.current_device())
+        _lib.preload(self.dev.index)
         self.mode = mode
         self.date = date or DateData(80.0 / 365.2425, 1950, 0, 1800.0)
         self.phys = SpeedyPhysics(parameters, diagnostics=False)
-        self.compute = torch.cuda.Stream(self.dev)
+        # tendency batches on the highest-priority stream: when an adjoint batch shares the
+        # GPU, the block scheduler hands freed SMs to tendency blocks first
+        self.compute = torch.cuda.Stream(self.dev, priority=-10)
         self.vjp_stream = torch.cuda.Stream(self.dev) if mode == "batched" else self.compute
         self.copy = torch.cuda.Stream(self.dev) if mode == "batched" else self.compute
         self._vg = {}
@@ -538,6 +666,10 @@ class CudaBackend:
             self.vjp_scratch = torch.empty(self._vjp_bytes, dtype=torch.uint8, device=self.dev)
         with torch.cuda.stream(self.compute):
             self.fwd_scratch = torch.empty(self._fwd_bytes, dtype=torch.uint8, device=self.dev)
+        self.arena = DeviceArena(self.dev, chunk_bytes=arena_chunk_bytes)
+        if reserve_bytes > 0:  # a service sizes its pool once, at startup
+            self.arena.reserve(reserve_bytes)
+        self.pinned = PinnedCache()
         self._t0 = None
         self._h0 = 0.0
 
@@ -596,61 +728,88 @@ class CudaBackend:
     def upload(self, h):
         torch = self.torch
         try:
-            with torch.cuda.stream(self.copy):
-                buf = torch.empty(h.nbytes, dtype=torch.uint8, device=self.dev)
-                buf.copy_(h.buffer, non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(self.copy)
+            buf, handle = self.arena.alloc(h.nbytes)
         except torch.cuda.OutOfMemoryError as e:
             raise MemoryError(str(e))
+        with torch.cuda.stream(self.copy):
+            buf[:h.nbytes].copy_(h.buffer, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.copy)
         base = buf.data_ptr()
         off, _ = member_layout(h.kx, h.ix, h.il)
         inputs = _lib.Inputs(**{n: base + off[n][0] for n in _lib.INPUT_FIELDS})
-        return _DevMember(h, buf, inputs, ev)
+        dm = _DevMember(h, buf, inputs, ev)
+        dm.handle = handle
+        return dm
 
     def release(self, dm):
+        self.arena.release(dm.handle)
         dm.buf = None
 
     def alloc_outputs(self, req, hosts):
-        torch = self.torch
-        stream = self.compute if req.kind == TENDENCY else self.vjp_stream
-        f = tendency_result_floats if req.kind == TENDENCY else vjp_result_floats
-        sizes = [_round_up(4 * f(h.kx, h.ix, h.il)) // 4 for h in hosts]
+        """One device buffer per request: every member's result planes, then (VJP) every
+        member's cotangent planes in one contiguous region, each region 256-byte aligned.  Only
+        offsets are recorded here; tensor views are made when results are read."""
+        if req.kind == TENDENCY:
+            names3 = ("u_wind", "v_wind", "temperature", "specific_humidity")
+            names2 = ("precnv", "precls")
+        else:
+            names3 = ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential")
+            names2 = ("normalized_surface_pressure",)
+        layout, pos = [], 0
+        for h in hosts:
+            c, kx = h.columns, h.kx
+            d, p = {}, pos
+            for k in names3:
+                d[k] = (p, (kx, h.ix, h.il))
+                p += kx * c
+            for k in names2:
+                d[k] = (p, (h.ix, h.il))
+                p += c
+            if req.kind == VJP:
+                d["params"] = (p, (12,))
+                p += 12
+            layout.append(d)
+            pos += _round_up(4 * (p - pos)) // 4
+        ct0 = pos
+        if req.kind == VJP:
+            for h, d in zip(hosts, layout):
+                c, kx = h.columns, h.kx
+                for k in ("u_wind", "v_wind", "temperature", "specific_humidity"):
+                    d["ct_" + k] = (pos, (kx, h.ix, h.il))
+                    pos += kx * c
+                pos = _round_up(4 * pos) // 4
         try:
-            with torch.cuda.stream(stream):
-                req._outputs = torch.empty(sum(sizes), dtype=torch.float32, device=self.dev)
-        except torch.cuda.OutOfMemoryError as e:
+            raw, req._out_handle = self.arena.alloc(4 * pos)
+        except self.torch.cuda.OutOfMemoryError as e:
             raise MemoryError(str(e))
-        views, pos = [], 0
-        for h, n in zip(hosts, sizes):
-            c, kx = h.ix * h.il, h.kx
-            o = req._outputs[pos:pos + n]
-            d, p = {}, 0
-            shape3, shape2 = (kx, h.ix, h.il), (h.ix, h.il)
-            if req.kind == TENDENCY:
-                names = [(k, shape3) for k in ("u_wind", "v_wind", "temperature",
-                                               "specific_humidity")]
-                names += [("precnv", shape2), ("precls", shape2)]
-            else:
-                names = [(k, shape3) for k in ("u_wind", "v_wind", "temperature",
-                                               "specific_humidity", "geopotential")]
-                names += [("normalized_surface_pressure", shape2), ("params", (12,))]
-                names += [("ct_" + k, shape3) for k in ("u_wind", "v_wind", "temperature",
-                                                        "specific_humidity")]
-            for k, shp in names:
-                m = int(np.prod(shp))
-                d[k] = o[p:p + m].view(shp)
-                p += m
-            views.append(d)
-            pos += n
-        req._views = views
+        req._outputs = raw[:4 * pos].view(self.torch.float32)
+        req._ct = req._outputs[ct0:] if req.kind == VJP else None
+        req._base = req._outputs.data_ptr()
+        req._views = layout
 
     def free_outputs(self, req):
+        h = req._out_handle
+        if h is not None:
+            self.arena.release(h)
+            req._out_handle = None
         req._outputs = None
         req._views = None
+        req._ct = None
 
     def results(self, req):
-        return req._views
+        """Per member, a dict of tensor views of its results (and cotangents, for a VJP)."""
+        out = req._outputs
+        res = []
+        for d in req._views:
+            v = {}
+            for k, (off, shape) in d.items():
+                n = 1
+                for x in shape:
+                    n *= x
+                v[k] = out[off:off + n].view(shape)
+            res.append(v)
+        return res
 
     # -- launches -------------------------------------------------------------------------------
     def launch(self, kind, reqs, devs):
@@ -669,92 +828,131 @@ class CudaBackend:
                     if id(dm) not in seen:
                         seen.add(id(dm))
                         stream.wait_event(dm.ready)
-                        dm.buf.record_stream(stream)
             start.record(stream)
-            if kind == VJP:
+            if kind == VJP and self.mode == "plain":
                 for r, dl in zip(reqs, devs):
-                    self._vjp(r, dl, stream)
+                    self._vjp_plain(r, dl, stream)
+            elif kind == VJP:
+                keep.append(self._vjp_batch(reqs, devs, stream))
             elif self.mode == "plain":
                 for r, dl in zip(reqs, devs):
-                    for dm, out in zip(dl, r._views):
-                        self._fwd_plain(dm, out, stream)
+                    for dm, d in zip(dl, r._views):
+                        self._fwd_plain(dm, r, d, stream)
             else:
                 keep.append(self._ensemble(reqs, devs, stream))
             done.record(stream)
         return _Handle(stream, start, done, keep)
 
-    def _outputs_struct(self, out):
-        return _lib.Outputs(**{k: (out[k].data_ptr() if k in out else None)
-                               for k in _lib.OUTPUT_FIELDS})
+    @staticmethod
+    def _ptrs(req, d, names):
+        return {k: (req._base + 4 * d[k][0] if k in d else None) for k in names}
 
-    def _fwd_plain(self, dm, out, stream):
+    def _outputs_struct(self, req, d):
+        return _lib.Outputs(**self._ptrs(req, d, _lib.OUTPUT_FIELDS))
+
+    def _fwd_plain(self, dm, req, d, stream):
         h = dm.host
         desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
         rc = self.lib.spd_fwd(C.byref(desc), C.byref(self.vgrid(h.kx)),
                               C.byref(self.phys._pstruct), C.byref(dm.inputs),
-                              C.byref(self._outputs_struct(out)),
+                              C.byref(self._outputs_struct(req, d)),
                               C.c_void_p(self.fwd_scratch.data_ptr()), self._fwd_bytes,
                               C.c_void_p(stream.cuda_stream))
         _lib.check(rc, "spd_fwd")
 
-    def _vjp(self, req, dl, stream):
-        torch = self.torch
-        for i, (dm, out) in enumerate(zip(dl, req._views)):
-            g = torch.Generator(device=self.dev)
-            g.manual_seed(int(req.seed) * 1009 + i)
-            for k in ("u_wind", "v_wind", "temperature", "specific_humidity"):
-                out["ct_" + k].normal_(generator=g)
+    def _cotangents(self, req):
+        """The request's cotangents: N(0, 1), one draw over its contiguous cotangent region from
+        a generator seeded by the request (so a request draws the same cotangents alone or in a
+        mix)."""
+        g = self.torch.Generator(device=self.dev)
+        g.manual_seed(int(req.seed))
+        req._ct.normal_(generator=g)
+
+    def _grads_struct(self, req, d):
+        return _lib.Grads(**self._ptrs(req, d, ("u_wind", "v_wind", "temperature",
+                                                "specific_humidity", "geopotential",
+                                                "normalized_surface_pressure", "params")))
+
+    def _ct_struct(self, req, d):
+        p = self._ptrs(req, d, ("ct_u_wind", "ct_v_wind", "ct_temperature",
+                                "ct_specific_humidity"))
+        return _lib.Cotangents(**{k[3:]: v for k, v in p.items()})
+
+    def _vjp_plain(self, req, dl, stream):
+        self._cotangents(req)
+        for dm, d in zip(dl, req._views):
             h = dm.host
             desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
-            cts = _lib.Cotangents(**{k: out["ct_" + k].data_ptr()
-                                     for k in ("u_wind", "v_wind", "temperature",
-                                               "specific_humidity")})
-            grads = _lib.Grads(**{k: out[k].data_ptr() for k in
-                                  ("u_wind", "v_wind", "temperature", "specific_humidity",
-                                   "geopotential", "normalized_surface_pressure", "params")})
             rc = self.lib.spd_vjp(C.byref(desc), C.byref(self.vgrid(h.kx)),
-                                  C.byref(self.phys._pstruct), C.byref(dm.inputs), C.byref(cts),
-                                  C.byref(grads), C.c_void_p(self.vjp_scratch.data_ptr()),
-                                  self._vjp_bytes, C.c_void_p(stream.cuda_stream))
+                                  C.byref(self.phys._pstruct), C.byref(dm.inputs),
+                                  C.byref(self._ct_struct(req, d)),
+                                  C.byref(self._grads_struct(req, d)),
+                                  C.c_void_p(self.vjp_scratch.data_ptr()), self._vjp_bytes,
+                                  C.c_void_p(stream.cuda_stream))
             _lib.check(rc, "spd_vjp")
 
-    def _ensemble(self, reqs, devs, stream):
-        torch = self.torch
+    def _classes(self, members):
         classes, cls_of = [], {}
-        members = []
-        for r, dl in zip(reqs, devs):
-            for dm, out in zip(dl, r._views):
-                h = dm.host
-                key = (h.kx, h.lfluxland)
-                if key not in cls_of:
-                    c = _lib.Class()
-                    c.desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
-                    c.vgrid = self.vgrid(h.kx)
-                    c.params = self.phys._pstruct
-                    cls_of[key] = len(classes)
-                    classes.append(c)
-                members.append((dm, out, cls_of[key]))
+        for h in members:
+            key = (h.kx, h.lfluxland)
+            if key not in cls_of:
+                c = _lib.Class()
+                c.desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+                c.vgrid = self.vgrid(h.kx)
+                c.params = self.phys._pstruct
+                cls_of[key] = len(classes)
+                classes.append(c)
         if len(classes) > _lib.MAX_CLASSES:
             raise ValueError("more member classes than one ensemble launch takes")
-        mem = (_lib.Member * len(members))()
-        for i, (dm, out, ci) in enumerate(members):
-            mem[i].inp = dm.inputs
-            mem[i].out = self._outputs_struct(out)
-            mem[i].ix, mem[i].il, mem[i].cls = dm.host.ix, dm.host.il, ci
-        cl = (_lib.Class * len(classes))(*classes)
-        nbytes = int(self.lib.spd_ensemble_plan_bytes(mem, len(members)))
-        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-        plan = torch.empty(nbytes, dtype=torch.uint8, device=self.dev)
+        return (_lib.Class * len(classes))(*classes), cls_of
+
+    def _plan(self, bytes_fn, plan_fn, classes, mem, n):
+        nbytes = int(bytes_fn(mem, n))
+        host = self.pinned.get(nbytes)
+        plan, handle = self.arena.alloc(nbytes)
         info = _lib.PlanInfo()
-        rc = self.lib.spd_ensemble_plan(cl, len(classes), mem, len(members),
-                                        C.c_void_p(host.data_ptr()),
-                                        C.c_void_p(plan.data_ptr()), nbytes, C.byref(info))
-        _lib.check(rc, "spd_ensemble_plan")
-        plan.copy_(host, non_blocking=True)
-        rc = self.lib.spd_ensemble_fwd(cl, len(classes), C.c_void_p(plan.data_ptr()),
-                                       C.byref(info), 0, C.c_void_p(stream.cuda_stream))
+        rc = plan_fn(classes, len(classes), mem, n, C.c_void_p(host.data_ptr()),
+                     C.c_void_p(plan.data_ptr()), nbytes, C.byref(info))
+        _lib.check(rc, "ensemble plan")
+        plan[:nbytes].copy_(host[:nbytes], non_blocking=True)
+        return host, handle, info
+
+    def _vjp_batch(self, reqs, devs, stream):
+        pairs = [(dm, r, d) for r, dl in zip(reqs, devs) for dm, d in zip(dl, r._views)]
+        for r in reqs:
+            self._cotangents(r)
+        cl, cls_of = self._classes([dm.host for dm, _, _ in pairs])
+        mem = (_lib.VjpMember * len(pairs))()
+        for i, (dm, r, d) in enumerate(pairs):
+            h = dm.host
+            mem[i].inp = dm.inputs
+            mem[i].ct = self._ct_struct(r, d)
+            mem[i].grads = self._grads_struct(r, d)
+            mem[i].ix, mem[i].il, mem[i].cls = h.ix, h.il, cls_of[(h.kx, h.lfluxland)]
+        host, handle, info = self._plan(self.lib.spd_ensemble_vjp_plan_bytes,
+                                        self.lib.spd_ensemble_vjp_plan, cl, mem, len(pairs))
+        plan = self.arena.chunks[handle[0]].data_ptr() + handle[1]
+        rc = self.lib.spd_ensemble_vjp(cl, len(cl), C.c_void_p(plan), C.byref(info), 0,
+                                       C.c_void_p(stream.cuda_stream))
+        _lib.check(rc, "spd_ensemble_vjp")
+        return (host, handle, cl, mem)
+
+    def _ensemble(self, reqs, devs, stream):
+        pairs = [(dm, r, d) for r, dl in zip(reqs, devs) for dm, d in zip(dl, r._views)]
+        cl, cls_of = self._classes([dm.host for dm, _, _ in pairs])
+        mem = (_lib.Member * len(pairs))()
+        for i, (dm, r, d) in enumerate(pairs):
+            h = dm.host
+            mem[i].inp = dm.inputs
+            mem[i].out = self._outputs_struct(r, d)
+            mem[i].ix, mem[i].il, mem[i].cls = h.ix, h.il, cls_of[(h.kx, h.lfluxland)]
+        host, handle, info = self._plan(self.lib.spd_ensemble_plan_bytes,
+                                        self.lib.spd_ensemble_plan, cl, mem, len(pairs))
+        plan = self.arena.chunks[handle[0]].data_ptr() + handle[1]
+        rc = self.lib.spd_ensemble_fwd(cl, len(cl), C.c_void_p(plan), C.byref(info), 0,
+                                       C.c_void_p(stream.cuda_stream))
         _lib.check(rc, "spd_ensemble_fwd")
-        return (host, plan, cl, mem)
+        return (host, handle, cl, mem)
 
     def done(self, handle):
         return handle.done.query()
@@ -769,4 +967,7 @@ class CudaBackend:
                 self._t0.elapsed_time(handle.done) / 1e3)
 
     def retire(self, handle):
+        for host, arena_handle, _, _ in handle.keep:
+            self.pinned.put(host)
+            self.arena.release(arena_handle)
         handle.keep = None

@@ -300,3 +300,75 @@ def test_latency_stats():
     assert st["p50_ms"] == pytest.approx(50.5, rel=1e-6)
     assert st["p99_ms"] == pytest.approx(99.01, rel=1e-6)
     assert st["columns"] == 1000
+
+
+def test_device_arena_best_fit_coalescing_and_growth():
+    import torch
+    made = []
+
+    def alloc(n):
+        made.append(n)
+        return torch.zeros(n, dtype=torch.uint8)
+
+    A = S.DeviceArena("cpu", chunk_bytes=1 << 20, alloc=alloc)
+    a, ha = A.alloc(1000)
+    b, hb = A.alloc(5000)
+    c, hc = A.alloc(300)
+    assert made == [1 << 20] and a.numel() == 1024 and b.numel() == 5120
+    offs = sorted(h[1] for h in (ha, hb, hc))
+    assert all(o % 256 == 0 for o in offs) and len(set(offs)) == 3
+    A.release(hb)
+    d, hd = A.alloc(4096)                      # best fit: reuses b's hole
+    assert hd[1] == hb[1]
+    A.release(ha)
+    A.release(hc)
+    A.release(hd)
+    assert A.free == [[[0, 1 << 20]]] and A.in_use == 0   # all coalesced back
+    big, hbig = A.alloc(3 << 20)               # larger than a chunk: a new chunk
+    assert len(made) == 2 and made[1] >= 3 << 20 and hbig[0] == 1
+    A.release(hbig)
+    e, he = A.alloc(100)
+    assert he[0] == 0                          # smallest fitting hole is in chunk 0
+
+
+def test_device_arena_reuse_never_overlaps():
+    import torch
+    rng = np.random.default_rng(1)
+    A = S.DeviceArena("cpu", chunk_bytes=1 << 22,
+                      alloc=lambda n: torch.zeros(n, dtype=torch.uint8))
+    live = {}
+    for step in range(400):
+        if live and rng.uniform() < 0.45:
+            k = list(live)[int(rng.integers(len(live)))]
+            A.release(live.pop(k))
+        else:
+            _, h = A.alloc(int(rng.integers(1, 200_000)))
+            live[step] = h
+        spans = sorted((h[0], h[1], h[1] + h[2]) for h in live.values())
+        for (c0, a0, b0), (c1, a1, b1) in zip(spans, spans[1:]):
+            assert c0 != c1 or b0 <= a1
+    for h in live.values():
+        A.release(h)
+    assert A.in_use == 0 and all(len(f) == 1 for f in A.free)
+
+
+def test_prefetch_makes_members_resident_within_budget():
+    hosts = dict(a=host(nbytes=1000), b=host(nbytes=1000), c=host(nbytes=1000))
+    be = FakeBackend()
+    sch = S.Scheduler(be, hosts.__getitem__, budget_bytes=2500)
+    assert sch.prefetch(["a", "b", "a"]) == 2
+    assert set(sch.resident) == {"a", "b"} and sch.used == 2000
+    assert sch.prefetch(["c"]) == 1            # evicts the least recently used idle member
+    assert "c" in sch.resident and len(sch.resident) == 2 and sch.used <= 2500
+    r = sch.submit(S.Request(S.TENDENCY, ["c"]))
+    assert r.status == "rejected"              # outputs do not fit beside any member
+
+
+def test_admission_is_capped_per_step():
+    src, _ = make_source(a=(8, 64, 32))
+    be = FakeBackend(per_col=1e-6)
+    sch = S.Scheduler(be, src, budget_bytes=1 << 30, max_admit_per_step=3)
+    for _ in range(7):
+        sch.submit(S.Request(S.TENDENCY, ["a"]))
+    sch.admit()
+    assert len(sch.waiting) == 4
