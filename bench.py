@@ -28,9 +28,16 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes (read + write) per column of the fused forward, from the committed ncu summaries
-# (profiles/); None until a capture exists for the workload.
-NCU_TRAFFIC_PER_COLUMN = {}
+# DRAM bytes (read + write) per column of the dominant kernel's launch, from one ncu capture
+# each (profiles/ensemble_columns_ragged_ensemble.md: 96.2 MB read + 48.9 MB written by one
+# ensemble_columns launch over 466,944 columns; profiles/column_kernel_k16_t425.md: 196.7 + 160.2
+# MB by column_kernel<16> over 819,200 columns).  Part of each launch's writes is still in L2 when
+# the kernel ends, so the write share reads low.
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.211456e6 + 48.920064e6) / 466944,
+                          "t425": (196.67712e6 + 160.18688e6) / 819200}
+# Warp instructions per launch of the dominant kernel (smsp__inst_executed.sum, same captures):
+# the compute side of the roofline, against one instruction per scheduler per cycle.
+NCU_WARP_INSTRUCTIONS = {"ensemble": 142825231.0, "t425": 306628651.0}
 
 
 def parse_args():
@@ -264,6 +271,17 @@ def run_b200(args):
                 "prepass_ms": (round(pre_ms, 4) if pre_ms is not None else None),
                 "algorithmic_bytes_per_launch": bytes_step,
                 "traffic": (round(traffic * cols) if traffic else None)}
+    # the bound that governs this kernel: instruction issue (one warp instruction per scheduler
+    # per cycle), with the instruction count of the ncu capture and the SM clock sampled here
+    insts = NCU_WARP_INSTRUCTIONS.get(args.workload)
+    issue = None
+    if insts and clk and world == 1:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak_issue = sms * 4 * clk["sm_mhz"] * 1e6
+        ach = insts / (kern_ms / 1e3)
+        issue = {"bound": "issue", "unit": "warp instructions/s", "achieved": round(ach, 1),
+                 "peak": round(peak_issue, 1), "frac": round(ach / peak_issue, 4),
+                 "warp_instructions_per_launch": insts, "sm_mhz": clk["sm_mhz"]}
 
     # end to end through the public API with host buffers (pinned), H2D + D2H timed
     e2e = None
@@ -315,7 +333,8 @@ def run_b200(args):
         del runs, ens
         torch.cuda.empty_cache()
         if "t425" in wanted:
-            sections["t425"] = t425_section(pkg, dev, peak, peak_kind)
+            sections["t425"] = t425_section(pkg, dev, peak, peak_kind,
+                                            clk["sm_mhz"] if clk else None)
         if "adjoint" in wanted:
             sections["adjoint"] = adjoint_section(pkg, dev)
         if "serving" in wanted:
@@ -328,7 +347,8 @@ def run_b200(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded generators with the workload's shapes and distributions)",
                 "config": workload_config(args.workload, members, args.mode),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+                "roofline": roofline, "issue_roofline": issue, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk,
                 "plain": plain, "grid_blocks": grid_blocks,
                 "gpu_launches": launches_per_step * args.steps}
         line.update(sections)
@@ -360,7 +380,7 @@ def event_ms(fn, reps, warmup=3):
     return a.elapsed_time(b) / reps
 
 
-def t425_section(pkg, dev, peak, peak_kind):
+def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
     """T425 (1280x640, 16 levels): the plain drop-in call, its column kernel timed alone, and 24
     consecutive calls captured in one CUDA graph."""
     import torch
@@ -405,7 +425,16 @@ def t425_section(pkg, dev, peak, peak_kind):
              "columns_per_s_plain": round(cols / (call_ms / 1e3), 1),
              "columns_per_s_graph": round(cols / (graph_ms / 1e3), 1),
              "column_kernel_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
-             "column_kernel_hbm_frac": round(bw / peak, 4)}
+             "column_kernel_hbm_frac": round(bw / peak, 4),
+             "column_kernel_traffic": round(NCU_TRAFFIC_PER_COLUMN["t425"] * cols)}
+    if sm_mhz:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak_issue = sms * 4 * sm_mhz * 1e6
+        ach = NCU_WARP_INSTRUCTIONS["t425"] / (col_ms / 1e3)
+        out_d["column_kernel_issue_frac"] = round(ach / peak_issue, 4)
+        out_d["issue_roofline_note"] = ("warp instructions per launch from ncu over one "
+                                        "instruction per scheduler per cycle at the sampled "
+                                        "SM clock")
     del g
     return out_d
 
