@@ -152,8 +152,10 @@ int spd_preload(void);
 /* derivative 0.5/0.5 (JAX's lax.min/lax.max rule); integer levels and the instance level set */
 /* carry no derivative.  With SPD_FUSE_VERIFY set the VJP is that of the fused step           */
 /* (verify_state, the physics, verify_tendencies and the humidity scale), and the humidity   */
-/* gradient is with respect to the humidity as given.  `scratch` holds the level-set word and  */
-/* the per-latitude solar table: spd_vjp_scratch_bytes(desc) bytes, 256-byte aligned.          */
+/* gradient is with respect to the humidity as given.  `scratch` holds a one-member plan (the  */
+/* instance's tile list, level-set word and per-latitude solar table), so that a single       */
+/* instance runs the batched adjoint's kernels: spd_vjp_scratch_bytes(desc) bytes, 256-byte   */
+/* aligned.                                                                                   */
 /* ----------------------------------------------------------------------------------------- */
 #define SPD_NUM_DIFF_PARAMS 12
 

@@ -10,7 +10,8 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libspeedy_b200.so")
+# SPEEDY_B200_LIB names another build of the library (e.g. a profiling variant).
+LIB_PATH = os.environ.get("SPEEDY_B200_LIB") or os.path.join(HERE, "libspeedy_b200.so")
 MAX_KX = 16
 
 SPD_LFLUXLAND = 1 << 0

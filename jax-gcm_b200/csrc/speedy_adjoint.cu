@@ -1,13 +1,13 @@
 // speedy_adjoint.cu -- the adjoint of the forward: one instance (spd_vjp) or a ragged ensemble
-// of them (spd_ensemble_vjp).
+// of them (spd_ensemble_vjp), both through the same two kernels.
 //
-// Launch 1 is the forward's cloud-top pre-pass (the instance level set S and the per-latitude
-// solar table: neither carries a derivative).  Launch 2 runs one thread per column: the
-// hand-written reverse pass of speedy_vjp.h recomputes the column's forward and walks its terms
-// backwards, writing the state gradients.  The 12 parameter gradients are summed per thread,
-// then per block, then with one atomicAdd per block and parameter.  The ensemble form runs both
-// launches over the tile list of speedy_ensemble.cuh; its blocks reduce per tile, into the
-// tile's member.
+// Launch 1 is the forward's cloud-top pre-pass over the tile list of speedy_ensemble.cuh (each
+// member's level set S and per-latitude solar table: neither carries a derivative).  Launch 2
+// runs one thread per column, one block per tile: the hand-written reverse pass of speedy_vjp.h
+// recomputes the column's forward and walks its terms backwards, writing the state gradients;
+// the 12 parameter gradients are summed per thread, then per block, then added to the tile's
+// member with one atomicAdd per parameter.  A single instance is a one-member plan written
+// into its scratch by a small kernel, so it runs exactly the ensemble's instructions.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -23,12 +23,7 @@ namespace spd {
 int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
-constexpr size_t kAdjHeader = 256;
 constexpr int kAdjBlock = 128;
-
-inline size_t vjp_scratch(const spd_desc_t* d) {
-  return kAdjHeader + align256((size_t)d->il * sizeof(ZonalRow));
-}
 
 struct VjpArgs {
   spd_vgrid_t vg;
@@ -39,11 +34,8 @@ struct VjpArgs {
 };
 
 // One column's VJP: loads, the reverse pass, stores; adds the parameter gradients to pacc.
-// Not inlined, so that the single-instance and ensemble kernels run the same instructions
-// (inlined, the compiler may contract multiply-adds differently in each caller) and give
-// bitwise-equal gradients.
 template <int KX>
-__device__ __noinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t& in,
+__device__ __forceinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t& in,
                                            const spd_cotangents_t& ct, const spd_grads_t& gr,
                                            uint32_t Sw, const ZonalRow* __restrict__ table,
                                            int c, int C, int il, float* pacc) {
@@ -116,20 +108,6 @@ __device__ __forceinline__ void block_add_params(float* pacc, float* params) {
   __syncthreads();
 }
 
-template <int KX>
-__global__ void __launch_bounds__(kAdjBlock, 3)
-    adjoint_kernel(const __grid_constant__ VjpArgs A, const spd_inputs_t in,
-                   const spd_cotangents_t ct, const spd_grads_t gr,
-                   const uint32_t* __restrict__ S, const ZonalRow* __restrict__ table) {
-  const uint32_t Sw = __ldg(S);
-  float pacc[SPD_NUM_DIFF_PARAMS];
-#pragma unroll
-  for (int j = 0; j < SPD_NUM_DIFF_PARAMS; ++j) pacc[j] = 0.0f;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < A.C; c += gridDim.x * blockDim.x)
-    vjp_column<KX>(A, in, ct, gr, Sw, table, c, A.C, A.il, pacc);
-  block_add_params(pacc, gr.params);
-}
-
 // ---- ensemble ----
 struct VjpMemberDev {
   spd_inputs_t in;
@@ -181,31 +159,50 @@ __global__ void __launch_bounds__(kAdjBlock, 3)
   }
 }
 
-template <int KX>
-static int launch_vjp(const VjpArgs& A, const Consts& K, const spd_inputs_t& in,
-                      const spd_cotangents_t& ct, const spd_grads_t& gr, char* scratch,
-                      cudaStream_t st) {
-  uint32_t* S = reinterpret_cast<uint32_t*>(scratch);
-  ZonalRow* table = reinterpret_cast<ZonalRow*>(scratch + kAdjHeader);
-  const int grid_a = (std::max(K.C, K.il) + kBlock - 1) / kBlock;
-  cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
-  const int grid = (A.C + kAdjBlock - 1) / kAdjBlock;
-  adjoint_kernel<KX><<<grid, kAdjBlock, 0, st>>>(A, in, ct, gr, S, table);
-  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+// The one-member plan of a single instance: its record and its tile list.
+__global__ void __launch_bounds__(kBlock) vjp_single_plan(const VjpMemberDev rec,
+                                                          VjpMemberDev* dst, Tile* tiles,
+                                                          int ntiles) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) *dst = rec;
+  for (; t < ntiles; t += gridDim.x * blockDim.x) tiles[t] = Tile{0, t * kNT};
+}
+
+struct OneMember {
+  int ix, il;
+};
+
+inline PlanLayout single_layout(const spd_desc_t* d) {
+  const OneMember m{d->ix, d->il};
+  return plan_layout(&m, 1, sizeof(VjpMemberDev));
 }
 
 int preload_adjoint() {
   cudaFuncAttributes a;
   bool ok = true;
-  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<7>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<8>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, adjoint_kernel<16>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<7>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<8>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<16>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, vjp_single_plan) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, ensemble_vjp_prepass) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, ensemble_adjoint) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
+}
+
+// Both launches over a plan already on the device (tiles at base + tiles_off).
+static int launch_ensemble_vjp(const ClassArgs& P, const VjpClassArgs& V, char* base,
+                               int nmembers, int ntiles, size_t levelset_offset,
+                               size_t levelset_bytes, int grid_blocks, cudaStream_t st) {
+  const VjpMemberDev* md = reinterpret_cast<const VjpMemberDev*>(base + 256);
+  const size_t tiles_off = 256 + align256((size_t)nmembers * sizeof(VjpMemberDev));
+  const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
+  // Default: one block per tile.  The blocks are short (one tile's columns each), so the SMs
+  // turn over often and a higher-priority stream's kernels (a forward batch) get them within
+  // one block's time; a persistent grid would hold every SM until the whole batch is done.
+  const int grid = grid_blocks > 0 ? std::min(grid_blocks, ntiles) : ntiles;
+  const int grid_pre = std::min(ntiles, 65535);
+  if (cudaMemsetAsync(base + levelset_offset, 0, levelset_bytes, st) != cudaSuccess)
+    return SPD_ERR_CUDA;
+  ensemble_vjp_prepass<<<grid_pre, kBlock, 0, st>>>(P, md, tl, ntiles);
+  ensemble_adjoint<<<grid, kAdjBlock, 0, st>>>(V, md, tl, ntiles);
+  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
 static VjpArgs make_vjp_args(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
@@ -248,7 +245,7 @@ extern "C" {
 
 size_t spd_vjp_scratch_bytes(const spd_desc_t* desc) {
   if (!desc || desc->ix <= 0 || desc->il <= 0) return 0;
-  return spd::vjp_scratch(desc);
+  return spd::single_layout(desc).total;
 }
 
 int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
@@ -258,22 +255,33 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
   if (!desc || !vgrid || !params || !in || !ct || !grads) return SPD_ERR_NULL;
   const int rc = check_vjp_member(desc, in, ct, grads);
   if (rc != SPD_OK) return rc;
-  if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) ||
-      scratch_bytes < vjp_scratch(desc))
+  const PlanLayout L = single_layout(desc);
+  if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) || scratch_bytes < L.total)
     return SPD_ERR_SCRATCH;
+  if (desc->kx != 7 && desc->kx != 8 && desc->kx != 16) return SPD_ERR_KX;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const Consts K = make_consts(desc, vgrid, params);
-  const VjpArgs A = make_vjp_args(desc, vgrid, params);
-  char* sc = static_cast<char*>(scratch);
-  if (cudaMemsetAsync(sc, 0, kAdjHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
-  if (cudaMemsetAsync(grads->params, 0, SPD_NUM_DIFF_PARAMS * sizeof(float), st) != cudaSuccess)
-    return SPD_ERR_CUDA;
-  switch (desc->kx) {
-    case 7: return launch_vjp<7>(A, K, *in, *ct, *grads, sc, st);
-    case 8: return launch_vjp<8>(A, K, *in, *ct, *grads, sc, st);
-    case 16: return launch_vjp<16>(A, K, *in, *ct, *grads, sc, st);
-    default: return SPD_ERR_KX;
-  }
+  char* base = static_cast<char*>(scratch);
+  ClassArgs P;
+  VjpClassArgs V;
+  P.cls[0].K = make_consts(desc, vgrid, params);
+  P.cls[0].D = derive_constants(desc, vgrid, params);
+  V.cls[0] = make_vjp_args(desc, vgrid, params);
+  VjpMemberDev rec;
+  rec.in = *in;
+  rec.ct = *ct;
+  rec.gr = *grads;
+  rec.C = desc->ix * desc->il;
+  rec.il = desc->il;
+  rec.kx = desc->kx;
+  rec.cls = 0;
+  rec.S = reinterpret_cast<uint32_t*>(base + L.levelset);
+  rec.table = reinterpret_cast<ZonalRow*>(base + L.tables);
+  VjpMemberDev* dst = reinterpret_cast<VjpMemberDev*>(base + L.members);
+  Tile* tiles = reinterpret_cast<Tile*>(base + L.tiles);
+  const int grid_init = std::min((L.ntiles + kBlock - 1) / kBlock, 1024);
+  vjp_single_plan<<<grid_init, kBlock, 0, st>>>(rec, dst, tiles, L.ntiles);
+  return launch_ensemble_vjp(P, V, base, 1, L.ntiles, L.levelset,
+                             align256(sizeof(uint32_t)), 0, st);
 }
 
 size_t spd_ensemble_vjp_plan_bytes(const spd_vjp_member_t* members, int nmembers) {
@@ -337,18 +345,9 @@ int spd_ensemble_vjp(const spd_class_t* classes, int nclasses, void* plan_device
   // Default: one block per tile.  The blocks are short (one tile's columns each), so the SMs
   // turn over often and a higher-priority stream's kernels (a forward batch) get them within
   // one block's time; a persistent grid would hold every SM until the whole batch is done.
-  int grid = grid_blocks > 0 ? std::min(grid_blocks, info->ntiles) : info->ntiles;
-  const int grid_pre = std::min(info->ntiles, 65535);
-  char* base = static_cast<char*>(plan_device);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const VjpMemberDev* md = reinterpret_cast<const VjpMemberDev*>(base + 256);
-  const size_t tiles_off = 256 + align256((size_t)info->nmembers * sizeof(VjpMemberDev));
-  const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
-  if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
-    return SPD_ERR_CUDA;
-  ensemble_vjp_prepass<<<grid_pre, kBlock, 0, st>>>(P, md, tl, info->ntiles);
-  ensemble_adjoint<<<grid, kAdjBlock, 0, st>>>(V, md, tl, info->ntiles);
-  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+  return launch_ensemble_vjp(P, V, static_cast<char*>(plan_device), info->nmembers,
+                             info->ntiles, info->levelset_offset, info->levelset_bytes,
+                             grid_blocks, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

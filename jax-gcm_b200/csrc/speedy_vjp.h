@@ -92,8 +92,12 @@ SPD_HD void radset_d(F temp, F epslw, F fb[4], F dfb[4]) {
 template <int KX, class F>
 struct Col {
   F t[KX], q[KX], phi[KX];
-  F qsat[KX], qs_t[KX], qs_p[KX], rh[KX], se[KX];
+  F qsat[KX];
   F dfl[KX];  // longwave flux divergence per level, all contributions
+  // relative humidity and dry static energy (humidity.py:44, convection.py:123), recomputed at
+  // each use rather than kept
+  SPD_HD F RH(int k) const { return q[k] / qsat[k]; }
+  SPD_HD F SE(int k) const { return F(1004.0) * t[k] + phi[k]; }
   F psa, u, v;
   F qdif;
   int ktop2, iptop_cv;
@@ -107,12 +111,20 @@ struct Col {
   F alb_l, albsfc, snowc;
 };
 
-// Adjoints.
+// Adjoints.  Those of RH = q / qsat and SE = 1004 T + phi are applied where they arise.
 template <int KX, class F>
 struct Bar {
-  F t[KX], q[KX], phi[KX], qsat[KX], rh[KX], se[KX];
+  F t[KX], q[KX], phi[KX], qsat[KX];
   F psa, u, v;
   F par[P_N];
+  SPD_HD void add_rh(const Col<KX, F>& c, int k, F v) {
+    q[k] += v / c.qsat[k];
+    qsat[k] -= v * (c.RH(k) / c.qsat[k]);
+  }
+  SPD_HD void add_se(int k, F v) {
+    t[k] += F(1004.0) * v;
+    phi[k] += v;
+  }
 };
 
 struct Ctx {
@@ -130,22 +142,19 @@ template <int KX, class F>
 SPD_HD void humidity(const Ctx& x, Col<KX, F>& c) {
   SPD_ROLL
   for (int k = 0; k < KX; ++k) {
-    c.qsat[k] = qsat_d(c.t[k], c.psa, F(x.vg->fsg[k]), c.qs_t[k], c.qs_p[k]);
-    c.rh[k] = c.q[k] / c.qsat[k];
-    c.se[k] = F(1004.0) * c.t[k] + c.phi[k];
+    F d_t, d_p;
+    c.qsat[k] = qsat_d(c.t[k], c.psa, F(x.vg->fsg[k]), d_t, d_p);
   }
 }
 
 template <int KX, class F>
-SPD_HD void humidity_rev(const Col<KX, F>& c, Bar<KX, F>& b) {
+SPD_HD void humidity_rev(const Ctx& x, const Col<KX, F>& c, Bar<KX, F>& b) {
   SPD_ROLL
   for (int k = 0; k < KX; ++k) {
-    const F rb = b.rh[k];
-    b.q[k] += rb / c.qsat[k];
-    const F qsb = b.qsat[k] - rb * (c.rh[k] / c.qsat[k]);
-    b.t[k] += F(1004.0) * b.se[k] + qsb * c.qs_t[k];
-    b.phi[k] += b.se[k];
-    b.psa += qsb * c.qs_p[k];
+    F d_t, d_p;
+    qsat_d(c.t[k], c.psa, F(x.vg->fsg[k]), d_t, d_p);
+    b.t[k] += b.qsat[k] * d_t;
+    b.psa += b.qsat[k] * d_p;
   }
 }
 
@@ -155,16 +164,16 @@ SPD_HD void humidity_rev(const Col<KX, F>& c, Bar<KX, F>& b) {
 template <int KX, class F>
 SPD_HD F mss2_at(const Ctx& x, const Col<KX, F>& c, int k) {
   if (k >= KX - 1) return F(0);
-  const F m0 = c.se[k] + F(2501.0) * c.qsat[k];
-  const F m1 = c.se[k + 1] + F(2501.0) * c.qsat[k + 1];
+  const F m0 = c.SE(k) + F(2501.0) * c.qsat[k];
+  const F m1 = c.SE(k + 1) + F(2501.0) * c.qsat[k + 1];
   return m0 + F(x.vg->wvi[k][1]) * (m1 - m0);
 }
 
 template <int KX, class F>
 SPD_HD void dconv(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c) {
-  const F mse0 = c.se[KX - 1] + F(2501.0) * c.q[KX - 1];
-  const F mse1 = vmin(mse0, c.se[KX - 2] + F(2501.0) * c.q[KX - 2]);
-  const F mss0 = vmax(mse0, c.se[KX - 1] + F(2501.0) * c.qsat[KX - 1]);
+  const F mse0 = c.SE(KX - 1) + F(2501.0) * c.q[KX - 1];
+  const F mse1 = vmin(mse0, c.SE(KX - 2) + F(2501.0) * c.q[KX - 2]);
+  const F mss0 = vmax(mse0, c.SE(KX - 1) + F(2501.0) * c.qsat[KX - 1]);
   int ktop1 = KX, ktop2 = KX;
   SPD_ROLL
   for (int k = KX - 4; k >= 2; --k) {
@@ -192,7 +201,7 @@ SPD_HD void dconv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c,
   F qthr0_b = F(0);
   const F qthr0 = g.rhbl * c.qsat[KX - 1];
   if (c.case1) {
-    const F mse0 = c.se[KX - 1] + F(2501.0) * c.q[KX - 1];
+    const F mse0 = c.SE(KX - 1) + F(2501.0) * c.q[KX - 1];
     const int j = c.ktop2 - 1;
     const F msthr = mss2_at(x, c, j);
     const F A = c.q[KX - 1] - qthr0;
@@ -203,14 +212,14 @@ SPD_HD void dconv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c,
     qthr0_b -= Ab;
     const F mse0_b = Bb * F(1.0 / 2501.0);
     const F msthr_b = -mse0_b;
-    b.se[KX - 1] += mse0_b;
+    b.add_se(KX - 1, mse0_b);
     b.q[KX - 1] += F(2501.0) * mse0_b;
     if (j < KX - 1) {
       const F w = F(x.vg->wvi[j][1]);
       const F m0b = msthr_b - w * msthr_b, m1b = w * msthr_b;
-      b.se[j] += m0b;
+      b.add_se(j, m0b);
       b.qsat[j] += F(2501.0) * m0b;
-      b.se[j + 1] += m1b;
+      b.add_se(j + 1, m1b);
       b.qsat[j + 1] += F(2501.0) * m1b;
     }
   } else if (c.case2) {
@@ -253,7 +262,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   w.sb3[0] = w.qb3[0] = F(0);
   SPD_ROLL
   for (int k = 1; k < KX; ++k) {
-    w.sb3[k] = c.se[k - 1] + F(vg.wvi[k - 1][1]) * (c.se[k] - c.se[k - 1]);
+    w.sb3[k] = c.SE(k - 1) + F(vg.wvi[k - 1][1]) * (c.SE(k) - c.SE(k - 1));
     w.qb3[k] = c.q[k - 1] + F(vg.wvi[k - 1][1]) * (c.q[k] - c.q[k - 1]);
   }
   w.sb = w.sb3[KX - 1];
@@ -264,7 +273,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   w.mn = vmin(F(5.0), w.ratio);
   w.fmass = w.fm0 * w.fpsa * w.mn;
   w.cbmf = mask ? w.fmass : F(0) * w.fmass;
-  w.fus = w.fmass * c.se[KX - 1];
+  w.fus = w.fmass * c.SE(KX - 1);
   w.fuq = w.fmass * w.qmax;
   w.fds = w.fmass * w.sb;
   w.fdq = w.fmass * w.qb;
@@ -275,7 +284,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
     F en = (k >= 1 && k <= KX - 2) ? w.entr[k] * c.psa * w.cbmf : F(0);
     en = lm ? en : F(0) * en;
     cm = cm + en * F(1.0);
-    cs = cs + en * c.se[k];
+    cs = cs + en * c.SE(k);
     cq = cq + en * c.q[k];
     w.fm3[k] = w.fmass + cm;
     w.fus3[k] = w.fus + cs;
@@ -329,7 +338,7 @@ SPD_HD void conv_tend(const Ctx& x, const Cv<KX, F>& w, F dt[KX], F dq[KX]) {
 }
 
 template <int KX, class F>
-SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, const Cv<KX, F>& w,
+SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<KX, F>& w,
                   const F* dt_b, const F* dq_b, F precnv_b, Bar<KX, F>& b) {
   const spd_vgrid_t& vg = *x.vg;
   const int iptop = c.iptop_cv;
@@ -418,8 +427,8 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, con
     const bool lm = (k <= KX - 2) && (k >= iptop);
     if (lm && k >= 1) {
       const F en = w.entr[k] * c.psa * w.cbmf;
-      const F en_b = CMB + CSB * c.se[k] + CQB * c.q[k];
-      b.se[k] += CSB * en;
+      const F en_b = CMB + CSB * c.SE(k) + CQB * c.q[k];
+      b.add_se(k, CSB * en);
       b.q[k] += CQB * en;
       const F ep = w.entr[k] * c.psa;
       cbmf_b += en_b * ep;
@@ -430,8 +439,8 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, con
       b.par[P_ENTMAX] += ep_b * c.psa * (e * e) / w.sentr;
     }
   }
-  fmass_b += fus_b * c.se[KX - 1] + fuq_b * w.qmax + fds_b * w.sb + fdq_b * w.qb;
-  b.se[KX - 1] += fus_b * w.fmass;
+  fmass_b += fus_b * c.SE(KX - 1) + fuq_b * w.qmax + fds_b * w.sb + fdq_b * w.qb;
+  b.add_se(KX - 1, fus_b * w.fmass);
   F qmax_b = fuq_b * w.fmass;
   F sb_b = fds_b * w.fmass;
   F qb_b = fdq_b * w.fmass;
@@ -461,8 +470,8 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, con
   SPD_ROLL
   for (int k = 1; k < KX; ++k) {
     const F ww = F(vg.wvi[k - 1][1]);
-    b.se[k - 1] += sb3_b[k] - ww * sb3_b[k];
-    b.se[k] += ww * sb3_b[k];
+    b.add_se(k - 1, sb3_b[k] - ww * sb3_b[k]);
+    b.add_se(k, ww * sb3_b[k]);
     b.q[k - 1] += qb3_b[k] - ww * qb3_b[k];
     b.q[k] += ww * qb3_b[k];
   }
@@ -574,14 +583,14 @@ template <int KX, class F>
 SPD_HD void clouds(const Ctx& x, Col<KX, F>& c, Cl<KX, F>& w, F fmask) {
   const spd_params_t& p = *x.p;
   const int nl1 = KX - 2;
-  w.m0 = c.rh[nl1] > F(p.rhcl1);
-  w.cloudc0 = w.m0 ? c.rh[nl1] - F(p.rhcl1) : F(0);
+  w.m0 = c.RH(nl1) > F(p.rhcl1);
+  w.cloudc0 = w.m0 ? c.RH(nl1) - F(p.rhcl1) : F(0);
   const int icl0 = w.m0 ? nl1 : KX;
   w.mk = 0u;
   w.cmax = F(0);
   SPD_ROLL
   for (int k = 2; k < KX - 2; ++k) {
-    const F drh = c.rh[k] - F(p.rhcl1);
+    const F drh = c.RH(k) - F(p.rhcl1);
     const bool m = drh > w.cloudc0 && c.q[k] > F(p.qacl);
     if (m) w.mk |= 1u << k;
     w.upd[k] = m ? drh : w.cloudc0;
@@ -594,7 +603,7 @@ SPD_HD void clouds(const Ctx& x, Col<KX, F>& c, Cl<KX, F>& w, F fmask) {
     const int cand = (w.cmax == w.upd[k]) ? (((w.mk >> k) & 1u) ? k : icl0) : icl0;
     icl = cand > icl ? cand : icl;
   }
-  w.gse = (c.se[KX - 2] - c.se[KX - 1]) / (c.phi[KX - 2] - c.phi[KX - 1]);
+  w.gse = (c.SE(KX - 2) - c.SE(KX - 1)) / (c.phi[KX - 2] - c.phi[KX - 1]);
   const F rrcl = F(1.0) / (F(p.rhcl2) - F(p.rhcl1));
   w.pr1v = F(86.4) * (c.precnv + c.precls);
   w.pr1 = vmin(F(p.pmaxcl), w.pr1v);
@@ -613,7 +622,7 @@ SPD_HD void clouds(const Ctx& x, Col<KX, F>& c, Cl<KX, F>& w, F fmask) {
   w.N = vmax(F(p.clsmax) - F(1.2) * cloudc, F(0.0));
   w.clstr1 = fstab * w.N;
   w.clstrl_m = vmax(w.clstr1, F(p.clsminl));
-  const F clstrl = w.clstrl_m * c.rh[KX - 1];
+  const F clstrl = w.clstrl_m * c.RH(KX - 1);
   c.clstr = w.clstr1 + fmask * (clstrl - w.clstr1);
 }
 
@@ -626,8 +635,8 @@ SPD_HD void clouds_rev(const Ctx& x, const Col<KX, F>& c, const Cl<KX, F>& w, F 
   // clstr = clstr1 + fmask (clstrl - clstr1); clstrl = max(clstr1, clsminl) rh[KX-1]
   F clstr1_b = clstr_b - fmask * clstr_b;
   const F clstrl_b = fmask * clstr_b;
-  b.rh[KX - 1] += clstrl_b * w.clstrl_m;
-  clstr1_b += clstrl_b * c.rh[KX - 1] * wmax(w.clstr1, F(p.clsminl));
+  b.add_rh(c, KX - 1, clstrl_b * w.clstrl_m);
+  clstr1_b += clstrl_b * c.RH(KX - 1) * wmax(w.clstr1, F(p.clsminl));
   // clstr1 = fstab * max(clsmax - 1.2 cloudc, 0)
   const F fstab = vmin(w.fstab_m, F(1.0));
   const F fstab_b = clstr1_b * w.N;
@@ -640,8 +649,8 @@ SPD_HD void clouds_rev(const Ctx& x, const Col<KX, F>& c, const Cl<KX, F>& w, F 
   const F den = c.phi[KX - 2] - c.phi[KX - 1];
   const F a_b = gse_b / den;
   const F d_b = -gse_b * (w.gse / den);
-  b.se[KX - 2] += a_b;
-  b.se[KX - 1] -= a_b;
+  b.add_se(KX - 2, a_b);
+  b.add_se(KX - 1, -(a_b));
   b.phi[KX - 2] += d_b;
   b.phi[KX - 1] -= d_b;
   b.q[nl1] += qcloud_b;
@@ -668,11 +677,11 @@ SPD_HD void clouds_rev(const Ctx& x, const Col<KX, F>& c, const Cl<KX, F>& w, F 
       ub = cmax_b;
     }
     if ((w.mk >> k) & 1u)
-      b.rh[k] += ub;
+      b.add_rh(c, k, ub);
     else
       cloudc0_b += ub;
   }
-  if (w.m0) b.rh[nl1] += cloudc0_b;
+  if (w.m0) b.add_rh(c, nl1, cloudc0_b);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -760,7 +769,7 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
 
 template <int KX, class F>
 SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c,
-                          const SurfaceRow& z, const Sw<KX, F>& w, const F* dt_b, F rsds_b,
+                          const SurfaceRow& z, Sw<KX, F>& w, const F* dt_b, F rsds_b,
                           F fsw0_b, F fsw1_b, F& cloudc_b, F& clstr_b, F& qcloud_b,
                           Bar<KX, F>& b) {
   const spd_vgrid_t& vg = *x.vg;
@@ -864,10 +873,14 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
 // ---------------------------------------------------------------------------------------------
 template <int KX, class F>
 struct Lw {
-  F tau[KX][4], st0[KX], st1[KX], th[KX];
   F fld[KX][4];      // downward pass: fluxes after level k
   F flu[KX + 1][4];  // upward pass: fluxes entering level k from below (flu[KX]: surface)
-  F s10, s11;
+};
+
+// One level's transmissivities and blackbody terms, recomputed wherever they are needed.
+template <class F>
+struct LwLevel {
+  F tau[4], st0, st1;
 };
 
 template <int KX, class F>
@@ -887,74 +900,83 @@ SPD_HD void lw_absorb(const Ctx& x, const Col<KX, F>& c, int k, F ablco2, F a[4]
   a[3] = a3;
 }
 
+// half-level temperature (longwave_radiation.py: interpolation to the layer interfaces)
 template <int KX, class F>
-SPD_HD void longwave_tables(const Ctx& x, const Col<KX, F>& c, F ablco2, Lw<KX, F>& w) {
-  const spd_vgrid_t& vg = *x.vg;
+SPD_HD F lw_th(const Ctx& x, const Col<KX, F>& c, int k) {
+  return c.t[k] + F(x.vg->wvi[k][1]) * (c.t[k + 1] - c.t[k]);
+}
+
+template <int KX, class F>
+SPD_HD void lw_level(const Ctx& x, const Col<KX, F>& c, int k, F ablco2, LwLevel<F>& L) {
+  F a[4];
+  lw_absorb(x, c, k, ablco2, a);
+  const F dh = F(x.vg->dhs[k]);
   SPD_ROLL
-  for (int k = 0; k < KX; ++k) {
-    F a[4];
-    lw_absorb(x, c, k, ablco2, a);
-    SPD_ROLL
-    for (int b = 0; b < 4; ++b) w.tau[k][b] = fexp(-a[b] * c.psa * F(vg.dhs[k]));
-  }
-  SPD_ROLL
-  for (int k = 0; k < KX - 1; ++k) w.th[k] = c.t[k] + F(vg.wvi[k][1]) * (c.t[k + 1] - c.t[k]);
-  w.s10 = F(0.75) * c.t[0] + F(0.25) * w.th[0];
-  w.s11 = F(0.50) * c.t[1] + F(0.25) * (w.th[0] + w.th[1]);
+  for (int b = 0; b < 4; ++b) L.tau[b] = fexp(-a[b] * c.psa * dh);
   const F sbc = F(5.67e-8);
-  w.st0[0] = sbc * ((w.s10 * w.s10) * (w.s10 * w.s10));
-  w.st1[0] = F(0);
-  w.st0[1] = sbc * ((w.s11 * w.s11) * (w.s11 * w.s11));
-  w.st1[1] = F(0);
-  SPD_ROLL
-  for (int k = 2; k < KX; ++k) {
-    const F grad = (k < KX - 1) ? F(0.5) * vmax(w.th[k] - w.th[k - 1], F(0.0))
-                                : vmax(c.t[KX - 1] - w.th[KX - 2], F(0.0));
+  if (k == 0) {
+    const F s10 = F(0.75) * c.t[0] + F(0.25) * lw_th(x, c, 0);
+    L.st0 = sbc * ((s10 * s10) * (s10 * s10));
+    L.st1 = F(0);
+  } else if (k == 1) {
+    const F s11 = F(0.50) * c.t[1] + F(0.25) * (lw_th(x, c, 0) + lw_th(x, c, 1));
+    L.st0 = sbc * ((s11 * s11) * (s11 * s11));
+    L.st1 = F(0);
+  } else {
+    const F grad = (k < KX - 1) ? F(0.5) * vmax(lw_th(x, c, k) - lw_th(x, c, k - 1), F(0.0))
+                                : vmax(c.t[KX - 1] - lw_th(x, c, KX - 2), F(0.0));
     const F st3 = sbc * (c.t[k] * c.t[k] * c.t[k]);
-    w.st0[k] = st3 * c.t[k];
-    w.st1[k] = F(4.0) * st3 * grad;
+    L.st0 = st3 * c.t[k];
+    L.st1 = F(4.0) * st3 * grad;
   }
 }
 
 template <int KX, class F>
-SPD_HD void longwave_down(const Ctx& x, Col<KX, F>& c, Lw<KX, F>& w) {
+SPD_HD void longwave_down(const Ctx& x, Col<KX, F>& c, F ablco2, Lw<KX, F>& w) {
   const spd_params_t& p = *x.p;
   F fb[4], dfb[4];
+  LwLevel<F> L;
+  lw_level(x, c, 0, ablco2, L);
   radset_d(c.t[0], F(p.epslw), fb, dfb);
   SPD_ROLL
   for (int b = 0; b < 4; ++b) {
-    const F emis = F(1) - w.tau[0][b];
-    w.fld[0][b] = emis * (fb[b] * (w.st0[0] + emis * w.st1[0]));
+    const F emis = F(1) - L.tau[b];
+    w.fld[0][b] = emis * (fb[b] * (L.st0 + emis * L.st1));
   }
   w.fld[0][2] = w.fld[0][3] = F(0);
   F sprev = ((w.fld[0][0] + w.fld[0][1]) + w.fld[0][2]) + w.fld[0][3];
   c.dfl[0] = F(0) + (-sprev);
+  F st0_last = L.st0;
   SPD_ROLL
   for (int k = 1; k < KX; ++k) {
+    lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
     SPD_ROLL
     for (int b = 0; b < 4; ++b) {
-      const F emis = F(1) - w.tau[k][b];
-      w.fld[k][b] = w.tau[k][b] * w.fld[k - 1][b] + emis * (fb[b] * (w.st0[k] + emis * w.st1[k]));
+      const F emis = F(1) - L.tau[b];
+      w.fld[k][b] = L.tau[b] * w.fld[k - 1][b] + emis * (fb[b] * (L.st0 + emis * L.st1));
     }
     const F sk = ((w.fld[k][0] + w.fld[k][1]) + w.fld[k][2]) + w.fld[k][3];
     c.dfl[k] = F(0) + (-(sk - sprev));
     sprev = sk;
+    st0_last = L.st0;
   }
   const F e = F(p.emisfc);
   const F* fl = w.fld[KX - 1];
   F rlds = ((e * fl[0] + e * fl[1]) + e * fl[2]) + e * fl[3];
-  const F corlw = F(p.epslw) * F(p.emisfc) * w.st0[KX - 1];
+  const F corlw = F(p.epslw) * F(p.emisfc) * st0_last;
   c.dfl[KX - 1] = c.dfl[KX - 1] + (-corlw);
   c.rlds = rlds + corlw;
 }
 
 template <int KX, class F>
-SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, Lw<KX, F>& w) {
+SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, F ablco2,
+                        Lw<KX, F>& w) {
   const spd_vgrid_t& vg = *x.vg;
   const spd_params_t& p = *x.p;
   const F refsfc = F(1) - F(p.emisfc);
   F fb[4], dfb[4];
+  LwLevel<F> L;
   radset_d(c.tsfc, F(p.epslw), fb, dfb);
   const F fsw[4] = {c.fsw0, c.fsw1, F(0), F(0)};
   SPD_ROLL
@@ -963,28 +985,32 @@ SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, Lw<KX,
   F sk = ((w.flu[KX][0] + w.flu[KX][1]) + w.flu[KX][2]) + w.flu[KX][3];
   SPD_ROLL
   for (int k = KX - 1; k >= 1; --k) {
+    lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
     SPD_ROLL
     for (int b = 0; b < 4; ++b) {
-      const F emis = F(1) - w.tau[k][b];
-      w.flu[k][b] = w.tau[k][b] * w.flu[k + 1][b] + emis * (fb[b] * (w.st0[k] - emis * w.st1[k]));
+      const F emis = F(1) - L.tau[b];
+      w.flu[k][b] = L.tau[b] * w.flu[k + 1][b] + emis * (fb[b] * (L.st0 - emis * L.st1));
     }
     const F skm1 = ((w.flu[k][0] + w.flu[k][1]) + w.flu[k][2]) + w.flu[k][3];
     c.dfl[k] = c.dfl[k] + (sk - skm1);
     sk = skm1;
   }
+  lw_level(x, c, 0, ablco2, L);
   radset_d(c.t[0], F(p.epslw), fb, dfb);
   F top[2];
   SPD_ROLL
   for (int b = 0; b < 2; ++b) {
-    const F emis = F(1) - w.tau[0][b];
-    top[b] = w.tau[0][b] * w.flu[1][b] + emis * (fb[b] * (w.st0[0] - emis * w.st1[0]));
+    const F emis = F(1) - L.tau[b];
+    top[b] = L.tau[b] * w.flu[1][b] + emis * (fb[b] * (L.st0 - emis * L.st1));
   }
   c.dfl[0] = c.dfl[0] + ((w.flu[1][0] - top[0]) + (w.flu[1][1] - top[1]));
+  LwLevel<F> L1;
+  lw_level(x, c, 1, ablco2, L1);
   const F eps1 = F(p.epslw) / (F(vg.dhs[0]) + F(vg.dhs[1]));
   const F stratc0 = F(z.stratz) * c.psa, stratc1 = eps1 * c.psa;
-  const F corlw1 = F(vg.dhs[0]) * stratc1 * w.st0[0] + stratc0;
-  const F corlw2 = F(vg.dhs[1]) * stratc1 * w.st0[1];
+  const F corlw1 = F(vg.dhs[0]) * stratc1 * L.st0 + stratc0;
+  const F corlw2 = F(vg.dhs[1]) * stratc1 * L1.st0;
   c.dfl[0] = c.dfl[0] + (-corlw1);
   c.dfl[1] = c.dfl[1] + (-corlw2);
 }
@@ -1008,158 +1034,175 @@ SPD_HD void lw_step_rev(F Ub, F tau, F uprev, F fb, F dfb, F st0, F st1, F sgn, 
   tau_b -= e_b;
 }
 
-// Adjoints shared by the two halves of the longwave reverse.
+// Applies the adjoints of level k's transmissivities and blackbody terms at once (they enter
+// linearly): to psa, q[k], T around level k and the two cloud absorption factors.
 template <int KX, class F>
-struct LwBar {
-  F dflb[KX], taub[KX][4], st0b[KX], st1b[KX];
-};
+SPD_HD void lw_level_rev(const Ctx& x, const Col<KX, F>& c, int k, F ablco2,
+                         const LwLevel<F>& L, const F tau_b[4], F st0_b, F st1_b, F& acl1_b,
+                         F& acl2_b, Bar<KX, F>& b) {
+  const spd_params_t& p = *x.p;
+  F a[4];
+  lw_absorb(x, c, k, ablco2, a);
+  const F dh = F(x.vg->dhs[k]);
+  F ab[4];
+  SPD_ROLL
+  for (int bb = 0; bb < 4; ++bb) {
+    const F Eb = tau_b[bb] * L.tau[bb];
+    ab[bb] = -Eb * c.psa * dh;
+    b.psa += -Eb * a[bb] * dh;
+  }
+  if (k >= 2 && k <= KX - 2) {
+    if (k > c.icltop)
+      acl1_b += ab[0];
+    else
+      acl2_b += ab[0];
+    const F acl2 = c.cloudc * F(p.ablcl2);
+    const F q1 = F(p.ablwv1) * c.q[k], q2 = F(p.ablwv2) * c.q[k];
+    b.q[k] += ab[2] * wmax(q1, acl2) * F(p.ablwv1) + ab[3] * wmax(q2, acl2) * F(p.ablwv2);
+    acl2_b += ab[2] * wmax(acl2, q1) + ab[3] * wmax(acl2, q2);
+  } else if (k > 0) {
+    b.q[k] += ab[2] * F(p.ablwv1) + ab[3] * F(p.ablwv2);
+  }
+  // blackbody terms; th_j = t_j + w_j (t_{j+1} - t_j)
+  const F sbc = F(5.67e-8);
+  auto add_th = [&](int j, F v) {
+    const F ww = F(x.vg->wvi[j][1]);
+    b.t[j] += v - ww * v;
+    b.t[j + 1] += ww * v;
+  };
+  if (k == 0) {
+    const F s10 = F(0.75) * c.t[0] + F(0.25) * lw_th(x, c, 0);
+    const F s10_b = st0_b * sbc * F(4) * (s10 * s10 * s10);
+    b.t[0] += F(0.75) * s10_b;
+    add_th(0, F(0.25) * s10_b);
+  } else if (k == 1) {
+    const F s11 = F(0.50) * c.t[1] + F(0.25) * (lw_th(x, c, 0) + lw_th(x, c, 1));
+    const F s11_b = st0_b * sbc * F(4) * (s11 * s11 * s11);
+    b.t[1] += F(0.50) * s11_b;
+    add_th(0, F(0.25) * s11_b);
+    add_th(1, F(0.25) * s11_b);
+  } else {
+    const F t = c.t[k];
+    const F st3 = sbc * (t * t * t);
+    const F dd = (k < KX - 1) ? lw_th(x, c, k) - lw_th(x, c, k - 1)
+                              : c.t[KX - 1] - lw_th(x, c, KX - 2);
+    const F grad = (k < KX - 1) ? F(0.5) * vmax(dd, F(0.0)) : vmax(dd, F(0.0));
+    const F st3_b = st0_b * t + st1_b * F(4.0) * grad;
+    b.t[k] += st0_b * st3 + st3_b * F(3) * sbc * t * t;
+    const F grad_b = st1_b * F(4.0) * st3;
+    const F d_b = grad_b * ((k < KX - 1) ? F(0.5) : F(1)) * wmax(dd, F(0.0));
+    if (k < KX - 1) {
+      add_th(k, d_b);
+      add_th(k - 1, -d_b);
+    } else {
+      b.t[KX - 1] += d_b;
+      add_th(KX - 2, -d_b);
+    }
+  }
+}
 
-// First half: the flux divergence's psa factor and the upward pass.  Gives the adjoints of the
-// surface's upward flux rlus2 and of the two shortwave fluxes the pass starts from.
+// First half of the longwave reverse: the flux divergence's psa factor and the upward pass.
+// Gives the adjoints of the surface's upward flux rlus2 and of the two shortwave fluxes the
+// pass starts from; adds the cloud factors' adjoints to acl1_b, acl2_b.
 template <int KX, class F>
 SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow& z,
-                            const Lw<KX, F>& w, const F* dt_b, LwBar<KX, F>& L, F& rlus2_b,
-                            F& fsw0_b, F& fsw1_b, Bar<KX, F>& b) {
+                            const Lw<KX, F>& w, F ablco2, const F* dt_b, F& rlus2_b, F& fsw0_b,
+                            F& fsw1_b, F& acl1_b, F& acl2_b, Bar<KX, F>& b) {
   const spd_vgrid_t& vg = *x.vg;
   const spd_params_t& p = *x.p;
+  auto dflb = [&](int k) { return dt_b[k] * F(vg.grdscp[k]) / c.psa; };
   SPD_ROLL
-  for (int k = 0; k < KX; ++k) {
-    L.dflb[k] = dt_b[k] * F(vg.grdscp[k]) / c.psa;
-    b.psa += -dt_b[k] * ((c.dfl[k] * F(vg.grdscp[k])) / c.psa) / c.psa;
-    L.st0b[k] = L.st1b[k] = F(0);
-    SPD_ROLL
-    for (int bb = 0; bb < 4; ++bb) L.taub[k][bb] = F(0);
-  }
+  for (int k = 0; k < KX; ++k) b.psa += -dt_b[k] * ((c.dfl[k] * F(vg.grdscp[k])) / c.psa) / c.psa;
+  F st0b_0, st0b_1;
   {
-    const F corlw1_b = -L.dflb[0], corlw2_b = -L.dflb[1];
+    const F corlw1_b = -dflb(0), corlw2_b = -dflb(1);
+    LwLevel<F> L0, L1;
+    lw_level(x, c, 0, ablco2, L0);
+    lw_level(x, c, 1, ablco2, L1);
     const F eps1 = F(p.epslw) / (F(vg.dhs[0]) + F(vg.dhs[1]));
     const F stratc1 = eps1 * c.psa;
-    const F stratc1_b = corlw1_b * F(vg.dhs[0]) * w.st0[0] + corlw2_b * F(vg.dhs[1]) * w.st0[1];
-    L.st0b[0] += corlw1_b * (F(vg.dhs[0]) * stratc1);
-    L.st0b[1] += corlw2_b * (F(vg.dhs[1]) * stratc1);
+    const F stratc1_b = corlw1_b * F(vg.dhs[0]) * L0.st0 + corlw2_b * F(vg.dhs[1]) * L1.st0;
+    st0b_0 = corlw1_b * (F(vg.dhs[0]) * stratc1);
+    st0b_1 = corlw2_b * (F(vg.dhs[1]) * stratc1);
     b.psa += corlw1_b * F(z.stratz) + stratc1_b * eps1;
   }
-  F Ub[4] = {L.dflb[0], L.dflb[0], F(0), F(0)};
+  F Ub[4] = {dflb(0), dflb(0), F(0), F(0)};
   F fb[4], dfb[4];
-  radset_d(c.t[0], F(p.epslw), fb, dfb);
-  SPD_ROLL
-  for (int bb = 0; bb < 2; ++bb) {
-    F ub_prev;
-    lw_step_rev(-L.dflb[0], w.tau[0][bb], w.flu[1][bb], fb[bb], dfb[bb], w.st0[0], w.st1[0],
-                F(-1), L.taub[0][bb], ub_prev, b.t[0], L.st0b[0], L.st1b[0]);
-    Ub[bb] += ub_prev;
+  LwLevel<F> L;
+  {
+    lw_level(x, c, 0, ablco2, L);
+    radset_d(c.t[0], F(p.epslw), fb, dfb);
+    F tb[4] = {F(0), F(0), F(0), F(0)};
+    F s0b = st0b_0, s1b = F(0);
+    SPD_ROLL
+    for (int bb = 0; bb < 2; ++bb) {
+      F ub_prev;
+      lw_step_rev(-dflb(0), L.tau[bb], w.flu[1][bb], fb[bb], dfb[bb], L.st0, L.st1, F(-1),
+                  tb[bb], ub_prev, b.t[0], s0b, s1b);
+      Ub[bb] += ub_prev;
+    }
+    lw_level_rev(x, c, 0, ablco2, L, tb, s0b, s1b, acl1_b, acl2_b, b);
   }
   SPD_ROLL
   for (int k = 1; k < KX; ++k) {
-    const F Sb = (k >= 2 ? L.dflb[k - 1] : F(0)) - L.dflb[k];
+    const F Sb = (k >= 2 ? dflb(k - 1) : F(0)) - dflb(k);
+    lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
+    F tb[4] = {F(0), F(0), F(0), F(0)};
+    F s0b = (k == 1) ? st0b_1 : F(0), s1b = F(0);
     SPD_ROLL
     for (int bb = 0; bb < 4; ++bb) {
       F nb;
-      lw_step_rev(Ub[bb] + Sb, w.tau[k][bb], w.flu[k + 1][bb], fb[bb], dfb[bb], w.st0[k],
-                  w.st1[k], F(-1), L.taub[k][bb], nb, b.t[k], L.st0b[k], L.st1b[k]);
+      lw_step_rev(Ub[bb] + Sb, L.tau[bb], w.flu[k + 1][bb], fb[bb], dfb[bb], L.st0, L.st1,
+                  F(-1), tb[bb], nb, b.t[k], s0b, s1b);
       Ub[bb] = nb;
     }
+    lw_level_rev(x, c, k, ablco2, L, tb, s0b, s1b, acl1_b, acl2_b, b);
   }
   const F refsfc = F(1) - F(p.emisfc);
   F fbs[4], dfbs[4];
   radset_d(c.tsfc, F(p.epslw), fbs, dfbs);
-  rlus2_b = L.dflb[KX - 1] * F(p.epslw);
+  rlus2_b = dflb(KX - 1) * F(p.epslw);
   SPD_ROLL
   for (int bb = 0; bb < 4; ++bb) {
-    const F u = Ub[bb] + L.dflb[KX - 1];
+    const F u = Ub[bb] + dflb(KX - 1);
     rlus2_b += u * fbs[bb];
     if (bb == 0) fsw0_b = u * refsfc;
     if (bb == 1) fsw1_b = u * refsfc;
   }
 }
 
-// Second half: the downward pass (given the adjoint of the surface's downward flux rlds), each
-// level's transmissivities and the blackbody fluxes.  Adds the adjoint of cloudc.
+// Second half: the downward pass (given the adjoint of the surface's downward flux rlds) with
+// each level's transmissivities and blackbody terms.
 template <int KX, class F>
 SPD_HD void longwave_rev_down(const Ctx& x, const Col<KX, F>& c, const Lw<KX, F>& w, F ablco2,
-                              LwBar<KX, F>& L, F rlds_b, F& cloudc_b, Bar<KX, F>& b) {
+                              const F* dt_b, F rlds_b, F& acl1_b, F& acl2_b, Bar<KX, F>& b) {
   const spd_vgrid_t& vg = *x.vg;
   const spd_params_t& p = *x.p;
-  const F corlw_b = rlds_b - L.dflb[KX - 1];
-  L.st0b[KX - 1] += corlw_b * (F(p.epslw) * F(p.emisfc));
+  auto dflb = [&](int k) { return dt_b[k] * F(vg.grdscp[k]) / c.psa; };
+  const F corlw_b = rlds_b - dflb(KX - 1);
   F Db[4];
   SPD_ROLL
   for (int bb = 0; bb < 4; ++bb) Db[bb] = rlds_b * F(p.emisfc);
-  F acl1_b = F(0), acl2_b = F(0);
   F fb[4], dfb[4];
+  LwLevel<F> L;
   SPD_ROLL
   for (int k = KX - 1; k >= 0; --k) {
-    const F Sb = -L.dflb[k] + (k < KX - 1 ? L.dflb[k + 1] : F(0));
+    const F Sb = -dflb(k) + (k < KX - 1 ? dflb(k + 1) : F(0));
+    lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
+    F tb[4] = {F(0), F(0), F(0), F(0)};
+    F s0b = (k == KX - 1) ? corlw_b * (F(p.epslw) * F(p.emisfc)) : F(0), s1b = F(0);
     const int nb_ = (k == 0) ? 2 : 4;
     SPD_ROLL
     for (int bb = 0; bb < nb_; ++bb) {
       F nb;
       const F prev = (k == 0) ? F(0) : w.fld[k - 1][bb];
-      lw_step_rev(Db[bb] + Sb, w.tau[k][bb], prev, fb[bb], dfb[bb], w.st0[k], w.st1[k], F(1),
-                  L.taub[k][bb], nb, b.t[k], L.st0b[k], L.st1b[k]);
+      lw_step_rev(Db[bb] + Sb, L.tau[bb], prev, fb[bb], dfb[bb], L.st0, L.st1, F(1), tb[bb],
+                  nb, b.t[k], s0b, s1b);
       Db[bb] = nb;
     }
-    // transmissivities of level k: tau = exp(-a psa dhs)
-    F a[4];
-    lw_absorb(x, c, k, ablco2, a);
-    const F dh = F(vg.dhs[k]);
-    F ab[4];
-    SPD_ROLL
-    for (int bb = 0; bb < 4; ++bb) {
-      const F Eb = L.taub[k][bb] * w.tau[k][bb];
-      ab[bb] = -Eb * c.psa * dh;
-      b.psa += -Eb * a[bb] * dh;
-    }
-    if (k >= 2 && k <= KX - 2) {
-      if (k > c.icltop)
-        acl1_b += ab[0];
-      else
-        acl2_b += ab[0];
-      const F acl2 = c.cloudc * F(p.ablcl2);
-      const F q1 = F(p.ablwv1) * c.q[k], q2 = F(p.ablwv2) * c.q[k];
-      b.q[k] += ab[2] * wmax(q1, acl2) * F(p.ablwv1) + ab[3] * wmax(q2, acl2) * F(p.ablwv2);
-      acl2_b += ab[2] * wmax(acl2, q1) + ab[3] * wmax(acl2, q2);
-    } else if (k > 0) {
-      b.q[k] += ab[2] * F(p.ablwv1) + ab[3] * F(p.ablwv2);
-    }
-  }
-  cloudc_b += acl1_b * F(p.ablcl1) + acl2_b * F(p.ablcl2);
-  // blackbody fluxes
-  const F sbc = F(5.67e-8);
-  F thb[KX];
-  SPD_ROLL
-  for (int k = 0; k < KX; ++k) thb[k] = F(0);
-  SPD_ROLL
-  for (int k = 2; k < KX; ++k) {
-    const F t = c.t[k];
-    const F st3 = sbc * (t * t * t);
-    const F dd = (k < KX - 1) ? w.th[k] - w.th[k - 1] : c.t[KX - 1] - w.th[KX - 2];
-    const F grad = (k < KX - 1) ? F(0.5) * vmax(dd, F(0.0)) : vmax(dd, F(0.0));
-    const F st3_b = L.st0b[k] * t + L.st1b[k] * F(4.0) * grad;
-    b.t[k] += L.st0b[k] * st3 + st3_b * F(3) * sbc * t * t;
-    const F grad_b = L.st1b[k] * F(4.0) * st3;
-    const F d_b = grad_b * ((k < KX - 1) ? F(0.5) : F(1)) * wmax(dd, F(0.0));
-    if (k < KX - 1) {
-      thb[k] += d_b;
-      thb[k - 1] -= d_b;
-    } else {
-      b.t[KX - 1] += d_b;
-      thb[KX - 2] -= d_b;
-    }
-  }
-  const F s10_b = L.st0b[0] * sbc * F(4) * (w.s10 * w.s10 * w.s10);
-  const F s11_b = L.st0b[1] * sbc * F(4) * (w.s11 * w.s11 * w.s11);
-  b.t[0] += F(0.75) * s10_b;
-  thb[0] += F(0.25) * s10_b + F(0.25) * s11_b;
-  b.t[1] += F(0.50) * s11_b;
-  thb[1] += F(0.25) * s11_b;
-  SPD_ROLL
-  for (int k = 0; k < KX - 1; ++k) {
-    const F ww = F(vg.wvi[k][1]);
-    b.t[k] += thb[k] - ww * thb[k];
-    b.t[k + 1] += ww * thb[k];
+    lw_level_rev(x, c, k, ablco2, L, tb, s0b, s1b, acl1_b, acl2_b, b);
   }
 }
 
@@ -1235,7 +1278,7 @@ SPD_HD void surface(const Ctx& x, Col<KX, F>& c, const SurfaceIn& s, const Surfa
   w.shf0 = chlcp * w.denv1 * (w.tskin - w.t1_0);
   const bool fh = F(p.fhum0) > F(0);
   w.qs10 = qsat_d(w.t1_0, c.psa, F(1), w.qs10_t, w.qs10_p);
-  w.q1_0 = fh ? F(p.fhum0) * (c.rh[KX - 1] * w.qs10) + (F(1) - F(p.fhum0)) * c.q[KX - 1]
+  w.q1_0 = fh ? F(p.fhum0) * (c.RH(KX - 1) * w.qs10) + (F(1) - F(p.fhum0)) * c.q[KX - 1]
               : c.q[KX - 1];
   w.qs00 = qsat_d(w.tskin, c.psa, F(1), w.qs00_t, w.qs00_p);
   w.Mv = F(s.soilw) * w.qs00 - w.q1_0;
@@ -1263,7 +1306,7 @@ SPD_HD void surface(const Ctx& x, Col<KX, F>& c, const SurfaceIn& s, const Surfa
                       : vmax(-F(p.dtheta), astab * (F(s.sst) - w.t2_1));
   w.denv2 = w.denv0 * (F(1) + w.dths_v * rdth);
   w.qs11 = qsat_d(w.t1_1, c.psa, F(1), w.qs11_t, w.qs11_p);
-  w.q1_1 = fh ? F(p.fhum0) * (c.rh[KX - 1] * w.qs11) + (F(1) - F(p.fhum0)) * c.q[KX - 1]
+  w.q1_1 = fh ? F(p.fhum0) * (c.RH(KX - 1) * w.qs11) + (F(1) - F(p.fhum0)) * c.q[KX - 1]
               : c.q[KX - 1];
   w.cdsdv = F(p.cds) * w.denv2;
   w.ustr1 = -w.cdsdv * c.u;
@@ -1334,8 +1377,8 @@ SPD_HD void surface_rev(const Ctx& x, const Col<KX, F>& c, const SurfaceIn& s,
   }
   const bool fh = F(p.fhum0) > F(0);
   if (fh) {
-    b.rh[KX - 1] += q1_1_b * F(p.fhum0) * w.qs11;
-    const F qs_b = q1_1_b * F(p.fhum0) * c.rh[KX - 1];
+    b.add_rh(c, KX - 1, q1_1_b * F(p.fhum0) * w.qs11);
+    const F qs_b = q1_1_b * F(p.fhum0) * c.RH(KX - 1);
     b.q[KX - 1] += q1_1_b * (F(1) - F(p.fhum0));
     t1_1_b += qs_b * w.qs11_t;
     b.psa += qs_b * w.qs11_p;
@@ -1393,8 +1436,8 @@ SPD_HD void surface_rev(const Ctx& x, const Col<KX, F>& c, const SurfaceIn& s,
   tskin_b += qs00_b * w.qs00_t;
   b.psa += qs00_b * w.qs00_p;
   if (fh) {
-    b.rh[KX - 1] += q1_0_b * F(p.fhum0) * w.qs10;
-    const F qs_b = q1_0_b * F(p.fhum0) * c.rh[KX - 1];
+    b.add_rh(c, KX - 1, q1_0_b * F(p.fhum0) * w.qs10);
+    const F qs_b = q1_0_b * F(p.fhum0) * c.RH(KX - 1);
     b.q[KX - 1] += q1_0_b * (F(1) - F(p.fhum0));
     t1_0_b += qs_b * w.qs10_t;
     b.psa += qs_b * w.qs10_p;
@@ -1504,8 +1547,8 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
   F tt[KX], qt[KX];
   SPD_ROLL
   for (int k = 0; k < KX; ++k) tt[k] = qt[k] = F(0);
-  const F dmse = c.se[KX - 1] - c.se[nl1 - 1] + F(2501.0) * (c.q[KX - 1] - c.qsat[nl1 - 1]);
-  const F drh = c.rh[KX - 1] - c.rh[nl1 - 1];
+  const F dmse = c.SE(KX - 1) - c.SE(nl1 - 1) + F(2501.0) * (c.q[KX - 1] - c.qsat[nl1 - 1]);
+  const F drh = c.RH(KX - 1) - c.RH(nl1 - 1);
   const F fcnv = (icnv > 0 && dmse >= F(0)) ? F(p.redshc) : F(1);
   if (dmse >= F(0)) {
     const F fluxse = fcnv * v.fshcse * dmse;
@@ -1527,7 +1570,7 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
     const bool cond = F(vg.hsg[k + 1]) > F(0.5);
     const F d0 = F(p.rhgrad) * (F(vg.fsg[k + 1]) - F(vg.fsg[k]));
     const F f2 = v.fvdiq * F(vg.hsg[k + 1]);
-    const F dr = c.rh[k + 1] - c.rh[k];
+    const F dr = c.RH(k + 1) - c.RH(k);
     fluxq[k] = (dr >= d0 && cond) ? f2 * c.qsat[k] * dr : F(0);
     qt[k] = qt[k] + fluxq[k] * (F(1) / F(vg.dhs[k]));
   }
@@ -1536,8 +1579,8 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
   F fse[KX];
   SPD_ROLL
   for (int k = 0; k < nl1; ++k) {
-    const F se0 = c.se[k + 1] - F(p.segrad) * (c.phi[k + 1] - c.phi[k]);
-    fse[k] = (c.se[k] < se0) ? v.fvdise * (se0 - c.se[k]) : F(0);
+    const F se0 = c.SE(k + 1) - F(p.segrad) * (c.phi[k + 1] - c.phi[k]);
+    fse[k] = (c.SE(k) < se0) ? v.fvdise * (se0 - c.SE(k)) : F(0);
     tt[k] = tt[k] + fse[k] * (F(1) / F(vg.dhs[k]));
   }
   F cum = F(0);
@@ -1567,11 +1610,11 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
   for (int k = nl1 - 1; k >= 0; --k) {
     acc += -dt_b[k + 1];
     const F fse_b = acc * (F(1) / (F(1) - F(vg.hsg[k + 1]))) + dt_b[k] * (F(1) / F(vg.dhs[k]));
-    const F se0 = c.se[k + 1] - F(p.segrad) * (c.phi[k + 1] - c.phi[k]);
-    if (c.se[k] < se0) {
+    const F se0 = c.SE(k + 1) - F(p.segrad) * (c.phi[k + 1] - c.phi[k]);
+    if (c.SE(k) < se0) {
       const F s_b = fse_b * v.fvdise;
-      b.se[k] -= s_b;
-      b.se[k + 1] += s_b;
+      b.add_se(k, -(s_b));
+      b.add_se(k + 1, s_b);
       b.phi[k + 1] -= s_b * F(p.segrad);
       b.phi[k] += s_b * F(p.segrad);
     }
@@ -1580,17 +1623,17 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
   for (int k = 2; k < KX - 2; ++k) {
     const bool cond = F(vg.hsg[k + 1]) > F(0.5);
     const F d0 = F(p.rhgrad) * (F(vg.fsg[k + 1]) - F(vg.fsg[k]));
-    const F dr = c.rh[k + 1] - c.rh[k];
+    const F dr = c.RH(k + 1) - c.RH(k);
     if (!(dr >= d0 && cond)) continue;
     const F f2 = v.fvdiq * F(vg.hsg[k + 1]);
     const F fl_b = dq_b[k] * (F(1) / F(vg.dhs[k])) - dq_b[k + 1] * (F(1) / F(vg.dhs[k + 1]));
     b.qsat[k] += fl_b * f2 * dr;
     const F dr_b = fl_b * f2 * c.qsat[k];
-    b.rh[k + 1] += dr_b;
-    b.rh[k] -= dr_b;
+    b.add_rh(c, k + 1, dr_b);
+    b.add_rh(c, k, -(dr_b));
   }
-  const F dmse = c.se[KX - 1] - c.se[nl1 - 1] + F(2501.0) * (c.q[KX - 1] - c.qsat[nl1 - 1]);
-  const F drh = c.rh[KX - 1] - c.rh[nl1 - 1];
+  const F dmse = c.SE(KX - 1) - c.SE(nl1 - 1) + F(2501.0) * (c.q[KX - 1] - c.qsat[nl1 - 1]);
+  const F drh = c.RH(KX - 1) - c.RH(nl1 - 1);
   const F fcnv = (icnv > 0 && dmse >= F(0)) ? F(p.redshc) : F(1);
   const F fq_b = dq_b[nl1 - 1] * (F(1) / F(vg.dhs[nl1 - 1])) -
                  dq_b[KX - 1] * (F(1) / F(vg.dhs[KX - 1]));
@@ -1607,12 +1650,12 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
     b.qsat[nl1 - 1] += fq_b * v.fvdiq2 * drh;
     drh_b = fq_b * v.fvdiq2 * c.qsat[nl1 - 1];
   }
-  b.se[KX - 1] += dmse_b;
-  b.se[nl1 - 1] -= dmse_b;
+  b.add_se(KX - 1, dmse_b);
+  b.add_se(nl1 - 1, -(dmse_b));
   b.q[KX - 1] += F(2501.0) * dmse_b;
   b.qsat[nl1 - 1] -= F(2501.0) * dmse_b;
-  b.rh[KX - 1] += drh_b;
-  b.rh[nl1 - 1] -= drh_b;
+  b.add_rh(c, KX - 1, drh_b);
+  b.add_rh(c, nl1 - 1, -(drh_b));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1657,27 +1700,31 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   for (int k = 0; k < KX; ++k) dq[k] = dt[k] = F(0);
   humidity(x, c);
   dconv(x, g, c);
-  {
-    Cv<KX, F> w;
-    conv(x, g, c, w);
-    c.precnv = w.precnv;
-    if (verify) conv_tend(x, w, dt, dq);
-  }
+  // The term internals share one scratch: convection and shortwave run (and are recomputed)
+  // outside the span in which the longwave fluxes are kept.  (The reverse passes keep their
+  // own work arrays as locals: addressed through pointers into this scratch, the device build
+  // corrupted one of them.)
+  union Scratch {
+    Cv<KX, F> cv;
+    Sw<KX, F> sw;
+    Lw<KX, F> lw;
+  } sc;
+  conv(x, g, c, sc.cv);
+  c.precnv = sc.cv.precnv;
+  if (verify) conv_tend(x, sc.cv, dt, dq);
   lsc(x, g, c, dt, dq);
   Cl<KX, F> cl;
   clouds(x, c, cl, F(in.fmask));
-  {
-    Sw<KX, F> w;
-    shortwave(x, g, c, z, w);
-  }
-  Lw<KX, F> lw;
-  longwave_tables(x, c, ablco2, lw);
-  longwave_down(x, c, lw);
+  shortwave(x, g, c, z, sc.sw);
+  Lw<KX, F>& lw = sc.lw;
+  longwave_down(x, c, ablco2, lw);
   Sf<F> sf;
   surface(x, c, s, z, sf);
-  longwave_up(x, c, z, lw);
+  longwave_up(x, c, z, ablco2, lw);
   // ---- cotangents of the physics tendencies ----
-  F dt_b[KX], dq_b[KX], qraw_b[KX];
+  const F* dt_b = ct_t;
+  F dq_b[KX];
+  uint32_t limited = 0u;  // levels where verify_tendencies replaced dq by -q / dt
   if (verify) {
     F du, dv;
     surface_tend<KX, F>(x, sf, dt, dq, du, dv);
@@ -1685,18 +1732,16 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   }
   SPD_ROLL
   for (int k = 0; k < KX; ++k) {
-    dt_b[k] = ct_t[k];
     F qb = ct_q[k] * q_tend_scale;
-    qraw_b[k] = F(0);
     if (verify && !(in.q[k] + dt_seconds * dq[k] >= F(0))) {
-      qraw_b[k] = -qb / dt_seconds;
+      limited |= 1u << k;
       qb = F(0);
     }
     dq_b[k] = qb;
   }
   SPD_ROLL
   for (int k = 0; k < KX; ++k)
-    b.t[k] = b.q[k] = b.phi[k] = b.qsat[k] = b.rh[k] = b.se[k] = F(0);
+    b.t[k] = b.q[k] = b.phi[k] = b.qsat[k] = F(0);
   b.psa = b.u = b.v = F(0);
   SPD_ROLL
   for (int j = 0; j < P_N; ++j) b.par[j] = F(0);
@@ -1706,33 +1751,27 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   // of the surface's upward flux, the surface gives that of the downward flux at the surface
   F rlus2_b = F(0), fsw0_b = F(0), fsw1_b = F(0), cloudc_b = F(0), rsds_b = F(0), rlds_b = F(0);
   {
-    LwBar<KX, F> L;
-    longwave_rev_up(x, c, z, lw, dt_b, L, rlus2_b, fsw0_b, fsw1_b, b);
+    F acl1_b = F(0), acl2_b = F(0);
+    longwave_rev_up(x, c, z, lw, ablco2, dt_b, rlus2_b, fsw0_b, fsw1_b, acl1_b, acl2_b, b);
     surface_rev(x, c, s, z, sf, ct_u, ct_v, dt_b[KX - 1], dq_b[KX - 1], rlus2_b, rsds_b,
                 rlds_b, b);
-    longwave_rev_down(x, c, lw, ablco2, L, rlds_b, cloudc_b, b);
+    longwave_rev_down(x, c, lw, ablco2, dt_b, rlds_b, acl1_b, acl2_b, b);
+    cloudc_b += acl1_b * F(p.ablcl1) + acl2_b * F(p.ablcl2);
   }
   F clstr_b = F(0), qcloud_b = F(0);
-  {
-    Sw<KX, F> w;
-    shortwave(x, g, c, z, w);
-    shortwave_rev(x, g, c, z, w, dt_b, rsds_b, fsw0_b, fsw1_b, cloudc_b, clstr_b, qcloud_b, b);
-  }
+  shortwave(x, g, c, z, sc.sw);
+  shortwave_rev(x, g, c, z, sc.sw, dt_b, rsds_b, fsw0_b, fsw1_b, cloudc_b, clstr_b, qcloud_b, b);
   F precnv_b = F(0), precls_b = F(0);
   clouds_rev(x, c, cl, F(in.fmask), cloudc_b, clstr_b, qcloud_b, precnv_b, precls_b, b);
   lsc_rev(x, g, c, dt_b, dq_b, precls_b, b);
-  F qdif_b;
-  {
-    Cv<KX, F> w;
-    conv(x, g, c, w);
-    qdif_b = conv_rev(x, g, c, w, dt_b, dq_b, precnv_b, b);
-  }
+  conv(x, g, c, sc.cv);
+  const F qdif_b = conv_rev(x, g, c, sc.cv, dt_b, dq_b, precnv_b, b);
   dconv_rev(x, g, c, qdif_b, b);
-  humidity_rev(c, b);
+  humidity_rev(x, c, b);
   SPD_ROLL
   for (int k = 0; k < KX; ++k) {
     const F qb = (verify && in.q[k] < F(0)) ? F(0) : b.q[k];
-    b.q[k] = qb + qraw_b[k];
+    b.q[k] = qb + (((limited >> k) & 1u) ? -(ct_q[k] * q_tend_scale) / dt_seconds : F(0));
   }
 }
 

@@ -2,9 +2,12 @@
 autograd through the torch op.
 
 The host float64 VJP is the finite-difference-checked one (tests/test_adjoint_cpu.py); the
-GPU computes in float32.  Bar: for each gradient field, normwise |gpu - host64| <= 1e-4 of the
-field's max over the columns whose integer diagnostics agree, after allowing for float32
-noise of the same size as the host float32 VJP's own distance from float64.
+GPU computes in float32.  Bar, per gradient field, column by column: |gpu - host64| <=
+max(1e-4, 3x the host float32 VJP's own largest distance from float64) of the field's max.  A
+column outside that bar is a branch flip (a convection, condensation or cloud threshold
+decided differently in float32) and is explained when the GPU agrees with the host float32
+VJP there, or when the host float32 VJP is itself outside the bar; at most 1 % of the columns
+may flip and none may be unexplained.
 """
 import importlib
 
@@ -72,9 +75,15 @@ def test_gpu_vjp_matches_host(pkg, host, kx):
         e_gpu = np.abs(g_gpu[k] - h64[k]) / scale
         e_32 = np.abs(h32[k] - h64[k]) / scale
         report[k] = (float(e_gpu.max()), float(e_32.max()))
-        # columns where float32 rounding flips a branch differ by O(1); allow a few
-        cols_bad = e_gpu.reshape(-1, inst.ix, inst.il).max(axis=0) > max(1e-4, 3 * e_32.max())
-        assert cols_bad.sum() <= max(2, 0.005 * inst.ix * inst.il), (k, report[k], cols_bad.sum())
+        # columns where float32 rounding flips a branch differ by O(1)
+        tol = max(1e-4, 3 * float(np.median(e_32.reshape(-1, inst.ix, inst.il).max(axis=0))))
+        colmax = lambda e: e.reshape(-1, inst.ix, inst.il).max(axis=0)
+        bad = colmax(e_gpu) > tol
+        agrees32 = colmax(np.abs(g_gpu[k] - h32[k]) / scale) <= tol
+        flips32 = colmax(e_32) > tol
+        unexplained = bad & ~agrees32 & ~flips32
+        assert unexplained.sum() == 0, (k, report[k], np.argwhere(unexplained))
+        assert bad.sum() <= max(2, 0.01 * inst.ix * inst.il), (k, report[k], bad.sum())
     print(inst.name, report)
     rel = np.abs(p_gpu - p64) / np.maximum(np.abs(p64), 1e-30)
     assert np.sum(rel > 1e-3) <= 1, (p_gpu, p64)
