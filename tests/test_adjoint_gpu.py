@@ -30,10 +30,10 @@ def host(tmp_path_factory):
     return build_host(tmp_path_factory.mktemp("hostcol") / "libhostcol.so")
 
 
-def _gpu_vjp(pkg, inst, cts):
+def _gpu_vjp(pkg, inst, cts, fuse_verify=False):
     import torch
     state, forcing, geom, date = pkg.instance_to_device(inst, "cuda")
-    phys = pkg.SpeedyPhysics(diagnostics=False)
+    phys = pkg.SpeedyPhysics(diagnostics=False, fuse_verify=fuse_verify, time_step=1800.0)
     t = lambda a: torch.as_tensor(a, dtype=torch.float32, device="cuda")
     cot = pkg.PhysicsTendency(t(cts["u"]), t(cts["v"]), t(cts["t"]), t(cts["q"]))
     gs, gp = pkg.adjoint.vjp(phys, state, forcing, geom, date, cot)
@@ -43,22 +43,38 @@ def _gpu_vjp(pkg, inst, cts):
                 psa=c(gs.normalized_surface_pressure), u=c(gs.u_wind), v=c(gs.v_wind)), c(gp)
 
 
-@pytest.mark.parametrize("kx", [8, 16])
-def test_gpu_vjp_matches_host(pkg, host, kx):
-    inst = pkg.synthetic.land_instance(700 + kx, 32, 16, kx)
-    tend, data, S = run_oracle(inst)
+CASES = [  # (kx, seed, lfluxland, fused verify with some negative humidity)
+    (8, 708, True, False), (16, 716, True, False), (7, 707, True, False),
+    (8, 808, False, False), (8, 908, True, True), (16, 916, True, True)]
+
+
+@pytest.mark.parametrize("kx,seed,lfluxland,verify", CASES)
+def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify):
+    inst = pkg.synthetic.land_instance(seed, 32, 16, kx)
+    inst.lfluxland = lfluxland
+    if verify:
+        mask = np.random.default_rng(seed).uniform(size=inst.q.shape) < 0.05
+        inst.q = np.where(mask, -np.abs(inst.q) * 0.01 - 1e-4, inst.q).astype(np.float32)
+    if verify:  # the level set and solar rows the GPU sees: those of the verified state
+        import copy
+        vinst = copy.deepcopy(inst)
+        vinst.q = np.where(vinst.q < 0, np.float32(0), vinst.q).astype(np.float32)
+        tend, data, S = run_oracle(vinst)
+    else:
+        tend, data, S = run_oracle(inst)
     vg, pr = structs(pkg, inst)
     rng = np.random.default_rng(kx)
     shape = (kx, inst.ix, inst.il)
     cts = dict(t=rng.normal(size=shape), q=rng.normal(size=shape), u=rng.normal(size=shape),
                v=rng.normal(size=shape))
-    g_gpu, p_gpu = _gpu_vjp(pkg, inst, cts)
+    g_gpu, p_gpu = _gpu_vjp(pkg, inst, cts, fuse_verify=verify)
+    flags = _flags(inst) | (16 if verify else 0)
     h64 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
     h32 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
     p64 = np.zeros(12)
     for i in range(inst.ix):
         for j in range(inst.il):
-            h = column_of(inst, data, S, i, j, _flags(inst))
+            h = column_of(inst, data, S, i, j, flags)
             ct = (list(cts["t"][:, i, j]) + [0.0] * (16 - kx),
                   list(cts["q"][:, i, j]) + [0.0] * (16 - kx),
                   float(cts["u"][-1, i, j]), float(cts["v"][-1, i, j]))
