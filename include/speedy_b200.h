@@ -17,6 +17,9 @@
  *  - Every call is asynchronous on `stream` (a cudaStream_t passed as void*), makes no host
  *    synchronisation and allocates no memory; scratch is caller-provided.
  *  - Return value 0 (SPD_OK) or one of the SPD_ERR_* codes; no exceptions cross the ABI.
+ *  - The forward's output fields overlap neither its input fields nor one another
+ *    (SPD_ERR_ALIAS): between its two launches the forward keeps intermediate per-column
+ *    values in its own output planes.
  */
 #ifndef SPEEDY_B200_H
 #define SPEEDY_B200_H
@@ -40,7 +43,8 @@ enum spd_status {
   SPD_ERR_CUDA = 5,      /* a CUDA launch or runtime call failed */
   SPD_ERR_DEVICE = 6,    /* the device reported an error status (bounded wait expired, ...) */
   SPD_ERR_ALIGN = 7,     /* a field pointer is not 16-byte aligned */
-  SPD_ERR_NOALLOC_LIMIT = 8 /* il above SPD_NOALLOC_MAX_IL for spd_fwd_noalloc */
+  SPD_ERR_NOALLOC_LIMIT = 8, /* il above SPD_NOALLOC_MAX_IL for spd_fwd_noalloc */
+  SPD_ERR_ALIAS = 9          /* an output field overlaps an input field or another output */
 };
 
 /* spd_desc_t.flags */

@@ -1,10 +1,14 @@
 // speedy_api.cu -- kernels and C-ABI entry points of the plain per-instance drop-in.
 //
-// spd_fwd runs two launches on the caller's stream:
-//   1. cloudtop_prepass: every column forms its cloud-top level clip(icltop, 0, kx-1) and the
-//      instance ORs them into one 32-bit level set S (the cross-column dependency of
-//      shortwave_radiation.py:62-68); the same launch writes the per-latitude solar table.
-//   2. column_kernel: the fused physics of every column (speedy_physics.py:88-127), reading S.
+// spd_fwd runs two launches on the caller's stream, together the fused physics of every
+// column (speedy_physics.py:88-127):
+//   1. moist_kernel: humidity, convection, large-scale condensation and clouds.  Every column
+//      forms its cloud-top level clip(icltop, 0, kx-1) and the instance ORs them into one
+//      32-bit level set S (the cross-column dependency of shortwave_radiation.py:62-68); the
+//      same launch writes the per-latitude solar table and stages the column's partial
+//      tendencies, qsat and cloud scalars in the output planes.
+//   2. column_kernel: radiation, surface fluxes and vertical diffusion, reading S and the
+//      stage, then verify_tendencies and every output.
 // One thread owns one column (speedy_kernels.cuh, speedy_column_smem.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -28,6 +32,51 @@ __global__ void __launch_bounds__(kNT, 4) column_kernel(const ConstsD CD, const 
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+namespace {
+struct Span {
+  uintptr_t lo, hi;  // [lo, hi)
+};
+Span span(const void* p, size_t n) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  return Span{a, a + n * sizeof(float)};
+}
+bool overlap(const Span& a, const Span& b) { return a.lo < b.hi && b.lo < a.hi; }
+}  // namespace
+
+// True when an output field overlaps an input field or another output field.
+static bool outputs_alias(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out) {
+  const size_t C = (size_t)d->ix * d->il, L = (size_t)d->kx * C;
+  const Span ins[] = {span(in->u_wind, L), span(in->v_wind, L), span(in->temperature, L),
+                      span(in->specific_humidity, L), span(in->geopotential, L),
+                      span(in->normalized_surface_pressure, C), span(in->alb0, C),
+                      span(in->sice_am, C), span(in->snowc_am, C), span(in->soilw_am, C),
+                      span(in->stl_am, C), span(in->sea_surface_temperature, C),
+                      span(in->fmask, C), span(in->orog, C), span(in->phis0, C),
+                      span(in->sia, d->il), span(in->coa, d->il)};
+  float* const diag[] = {out->cbmf, out->cloudc, out->cloudstr, out->rsds, out->rsns,
+                         out->ftop_sw, out->rlds, out->rlns, out->ftop_lw, out->tsfc,
+                         out->tskin, out->shf, out->evap};
+  Span outs[6 + 13 + 2];
+  int n = 0;
+  outs[n++] = span(out->u_wind, L);
+  outs[n++] = span(out->v_wind, L);
+  outs[n++] = span(out->temperature, L);
+  outs[n++] = span(out->specific_humidity, L);
+  outs[n++] = span(out->precnv, C);
+  outs[n++] = span(out->precls, C);
+  for (float* p : diag)
+    if (p) outs[n++] = span(p, C);
+  if (out->iptop) outs[n++] = span(out->iptop, C);
+  if (out->icltop) outs[n++] = span(out->icltop, C);
+  for (int i = 0; i < n; ++i) {
+    for (const Span& a : ins)
+      if (overlap(outs[i], a)) return true;
+    for (int j = 0; j < i; ++j)
+      if (overlap(outs[i], outs[j])) return true;
+  }
+  return false;
+}
+
 int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out) {
   if (!d || !in || !out) return SPD_ERR_NULL;
   if (d->kx != 7 && d->kx != 8 && d->kx != 16) return SPD_ERR_KX;
@@ -43,6 +92,15 @@ int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_output
   for (const void* p : req)
     if (!aligned16(p)) return SPD_ERR_ALIGN;
   return SPD_OK;
+}
+
+// check_instance plus the forward's own rule: its outputs overlap neither its inputs nor one
+// another (the first launch stages values in the output planes that the second reads back).
+int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
+                           const spd_outputs_t* out) {
+  const int rc = check_instance(d, in, out);
+  if (rc != SPD_OK) return rc;
+  return outputs_alias(d, in, out) ? SPD_ERR_ALIAS : SPD_OK;
 }
 
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p) {
@@ -72,9 +130,8 @@ static int launch_fwd(const ConstsD& CD, const spd_inputs_t& in, const spd_outpu
     attr_done = true;
   }
   const Consts& K = CD.K;
-  const int grid = (K.C + kNT - 1) / kNT;
-  const int grid_a = (max(K.C, K.il) + kBlock - 1) / kBlock;
-  cloudtop_prepass<KX><<<grid_a, kBlock, 0, st>>>(K, in, S, table);
+  const int grid = (K.C + kNT - 1) / kNT;  // C = ix * il >= il covers the solar table too
+  moist_kernel<KX><<<grid, kNT, 0, st>>>(CD, in, out, S, table);
   if (marker && cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
   column_kernel<KX><<<grid, kNT, smem_bytes<KX>(), st>>>(CD, in, out, S, table);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
@@ -100,9 +157,9 @@ static int preload_api() {
   ok &= cudaFuncGetAttributes(&a, column_kernel<7>) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, column_kernel<8>) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, column_kernel<16>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<7>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<8>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, cloudtop_prepass<16>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, moist_kernel<7>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, moist_kernel<8>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, moist_kernel<16>) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 
@@ -133,7 +190,7 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
                    const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
                    size_t scratch_bytes, void* stream, void* event) {
-  int rc = spd::check_instance(desc, in, out);
+  int rc = spd::check_forward_instance(desc, in, out);
   if (rc != SPD_OK) return rc;
   if (!vgrid || !params) return SPD_ERR_NULL;
   if (!scratch || (reinterpret_cast<uintptr_t>(scratch) & 255u) ||
@@ -164,6 +221,7 @@ const char* spd_status_string(int status) {
     case SPD_ERR_NOALLOC_LIMIT:
       return "instance has more latitudes than spd_fwd_noalloc's fixed scratch holds "
              "(SPD_NOALLOC_MAX_IL)";
+    case SPD_ERR_ALIAS: return "an output field overlaps an input field or another output";
     default: return "unknown status";
   }
 }

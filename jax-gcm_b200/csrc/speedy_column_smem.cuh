@@ -12,6 +12,11 @@
 // absorbed fluxes are added to the temperature accumulator as each piece completes, and the
 // vertical-diffusion terms are formed level by level in one ascending pass.
 //
+// The column is split in two halves, run by two launches: column_first (humidity through
+// clouds) ends at the cloud-top level, the one cross-column dependency; column_second
+// (radiation, surface fluxes, vertical diffusion) needs the instance's level set of cloud tops
+// and resumes from what the first half left (qsat, the tendency accumulators, a few scalars).
+//
 // Expression order follows the reference term by term (file:line relative to the JAX-GCM
 // root).  Deviations, all at the rounding level and never inside a cancelling difference:
 // final scalings by 1/psa use one reciprocal, and the radiative absorbed-flux pieces of a
@@ -37,6 +42,7 @@ template <int KX>
 constexpr size_t smem_bytes() {
   return (size_t)kNumArrays * KX * kNT * sizeof(float);
 }
+
 
 struct ConstsD {
   Consts K;
@@ -90,34 +96,35 @@ __device__ __forceinline__ void radset_w(float temp, float w, float fb[4]) {
   fb[3] = w * f3;
 }
 
+// First half of the column: humidity, convection, large-scale condensation and clouds, with
+// every level loop fully unrolled so that the level arrays live in registers.  In: the state T,
+// Q (clamped by the caller where verify applies), PHI, and s.psa, s.fmask.  Out: qsat QS, the
+// convective + condensation tendency accumulators DT and DQ, and in o the convective and
+// cloud results (iptop, icltop, cbmf, precnv, precls, cloudc, clstr).
 template <int KX>
-__device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, const ZonalRow& z,
-                            uint32_t S, ColScalars& o) {
+__device__ __forceinline__ void column_first(const ConstsD& C, const float (&T)[KX],
+                                             const float (&Q)[KX], const float (&PHI)[KX],
+                                             const SurfaceIn& s, float (&QS)[KX],
+                                             float (&DT)[KX], float (&DQ)[KX], ColScalars& o) {
   const Consts& K = C.K;
   const Derived& D = C.D;
   const spd_params_t& p = K.p;
   const spd_vgrid_t& vg = K.vg;
-  const int tid = threadIdx.x;
-  auto arr = [&](int a) { return Lv{sm + (size_t)a * KX * kNT + tid}; };
-  const Lv T = arr(A_T), Q = arr(A_Q), PHI = arr(A_PHI), QS = arr(A_QSAT), DT = arr(A_DT),
-           DQ = arr(A_DQ), W = arr(A_W);
   auto rh_at = [&](int k) { return Q[k] / QS[k]; };  // spec_hum_to_rel_hum (humidity.py:45)
   const float psa = s.psa;
   const float rps = 1.0f / psa;
+  float SE[KX];  // dry static energy cp T + phi
 
   // ---- spec_hum_to_rel_hum (humidity.py:16-51) --------------------------------------------
-#pragma unroll 4
-  for (int k = 0; k < KX; ++k) QS[k] = qsat_of(T[k], psa, vg.fsg[k]);
-
-  // ---- set_forcing (physics/speedy/forcing.py:11-39) --------------------------------------
-  const float snowc = fminf(1.0f, s.snowc);
-  const float alb_l = s.alb0 + snowc * (p.albsn - s.alb0);
-  const float alb_s = p.albsea + s.sice * (p.albice - p.albsea);
-  const float albsfc = alb_s + s.fmask * (alb_l - alb_s);
+#pragma unroll
+  for (int k = 0; k < KX; ++k) {
+    QS[k] = qsat_of(T[k], psa, vg.fsg[k]);
+    SE[k] = kCp * T[k] + PHI[k];
+  }
 
   // ---- diagnose_convection (convection.py:15-97) -------------------------------------------
   const float q_b = Q[KX - 1], q_b1 = Q[KX - 2];
-  const float se_b = se_at(T, PHI, KX - 1), se_b1 = se_at(T, PHI, KX - 2);
+  const float se_b = SE[KX - 1], se_b1 = SE[KX - 2];
   int iptop;
   float qdif = 0.0f;
   {
@@ -127,10 +134,10 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
     const float mss0 = fmaxf(mse0, se_b + kAlhc * QS[KX - 1]);
     int ktop1 = KX, ktop2 = KX;
     float msthr = 0.0f;
-    float mk1 = se_at(T, PHI, KX - 3) + kAlhc * QS[KX - 3];
-#pragma unroll 1
+    float mk1 = SE[KX - 3] + kAlhc * QS[KX - 3];
+#pragma unroll
     for (int k = KX - 4; k >= 2; --k) {
-      const float mk = se_at(T, PHI, k) + kAlhc * QS[k];
+      const float mk = SE[k] + kAlhc * QS[k];
       const float mss2 = mk + vg.wvi[k][1] * (mk1 - mk);
       if (mss0 > mss2) ktop1 = k + 1;
       if (mse1 > mss2) {
@@ -166,7 +173,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
     float fm_n = 0.f, fus_n = 0.f, fuq_n = 0.f, fds_n = 0.f, fdq_n = 0.f;
     float dfqa_last = 0.0f, precnv = 0.0f;
     float se_k = se_b, q_k = q_b;
-#pragma unroll 1
+#pragma unroll
     for (int k = KX - 1; k >= 0; --k) {
       const bool lm = (k <= KX - 2) && (k >= iptop);
       float en = (k >= 1 && k <= KX - 2) ? D.entr[k] * psa * cbmf : 0.0f;
@@ -177,7 +184,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
       const float fm_k = fmass + cm, fus_k = fus + cs, fuq_k = fuq + cq;
       float se_m = 0.0f, q_m = 0.0f, fds_k, fdq_k;
       if (k >= 1) {
-        se_m = se_at(T, PHI, k - 1);
+        se_m = SE[k - 1];
         q_m = Q[k - 1];
       }
       if (k == KX - 1) {
@@ -241,7 +248,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
     const float psa2 = psa * psa;
     float psum = 0.0f;
     int first = 0;
-#pragma unroll 2
+#pragma unroll
     for (int k = 1; k < KX; ++k) {
       const float dqa = D.rhref[k] * QS[k] - Q[k];
       float dql = 0.0f, dtl = 0.0f;
@@ -273,7 +280,7 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
     // upd_k == cmax (i.e. all m_k and min upd == max upd), and icl0 otherwise: one pass.
     float cmax = -INFINITY, cmin = INFINITY;
     bool allm = true;
-#pragma unroll 1
+#pragma unroll
     for (int k = 2; k < KX - 2; ++k) {
       const float drh = rh_at(k) - p.rhcl1;
       const bool m = (drh > cloudc0) && (Q[k] > p.qacl);
@@ -297,6 +304,33 @@ __device__ void column_smem(const ConstsD& C, float* sm, const SurfaceIn& s, con
   o.cloudc = cloudc;
   o.clstr = clstr;
   o.icltop = icltop;
+}
+
+// Second half: shortwave, longwave, surface fluxes and vertical diffusion, from the state, qsat
+// and tendency accumulators in shared memory and the first half's results in o.
+template <int KX>
+__device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, const ZonalRow& z,
+                              uint32_t S, ColScalars& o) {
+  const Consts& K = C.K;
+  const Derived& D = C.D;
+  const spd_params_t& p = K.p;
+  const spd_vgrid_t& vg = K.vg;
+  const int tid = threadIdx.x;
+  auto arr = [&](int a) { return Lv{sm + (size_t)a * KX * kNT + tid}; };
+  const Lv T = arr(A_T), Q = arr(A_Q), PHI = arr(A_PHI), QS = arr(A_QSAT), DT = arr(A_DT),
+           DQ = arr(A_DQ), W = arr(A_W);
+  auto rh_at = [&](int k) { return Q[k] / QS[k]; };  // spec_hum_to_rel_hum (humidity.py:45)
+  const float psa = s.psa;
+  const float rps = 1.0f / psa;
+  const float snowc = fminf(1.0f, s.snowc);
+  const float alb_l = s.alb0 + snowc * (p.albsn - s.alb0);
+  const float alb_s = p.albsea + s.sice * (p.albice - p.albsea);
+  const float albsfc = alb_s + s.fmask * (alb_l - alb_s);
+  const float q_b = Q[KX - 1];
+  const float se_b = se_at(T, PHI, KX - 1), se_b1 = se_at(T, PHI, KX - 2);
+  const int iptop = o.iptop;
+  const float cloudc = o.cloudc, clstr = o.clstr, qcloud = Q[KX - 2];
+  const int icltop = o.icltop;
 
   // ---- shortwave_rad_fluxes (shortwave_radiation.py:27-217); W = reflection tau2[:,2] -------
   float flux_sw0, flux_sw1, rsds;

@@ -4,10 +4,11 @@
 // A member is one grid instance (its own arrays, ix*il columns, kx levels).  The plan splits
 // every member into tiles of kNT consecutive columns (a tile never straddles members), ordered
 // by level count (16-level tiles first, the heavier work), and keeps per member the field
-// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 is the
-// cloud-top pre-pass over all tiles (each member's level set and solar table, as in
-// spd_fwd's first launch); launch 2 runs the full column body on all tiles, reading each
-// member's level set.  Both launches are persistent: gridDim blocks stride over the tile list.
+// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 runs the
+// first half of every column on all tiles (each member's level set, solar table and staged
+// values, as in spd_fwd's first launch); launch 2 runs the second half on all tiles, reading
+// each member's level set.  Both launches are persistent: gridDim blocks stride over the tile
+// list.
 // Constants shared by a class of members (kx, date, switches, vertical grid, parameters) travel
 // by value in the kernel parameters.
 #include <cuda_runtime.h>
@@ -21,14 +22,30 @@
 
 namespace spd {
 
-int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
+int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
+                           const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
-__global__ void __launch_bounds__(kBlock) ensemble_prepass(const __grid_constant__ ClassArgs A,
-                                                           const MemberDev* __restrict__ members,
-                                                           const Tile* __restrict__ tiles,
-                                                           int ntiles) {
-  prepass_tiles(A, members, tiles, ntiles);
+__global__ void __launch_bounds__(kNT, 5) ensemble_moist(const __grid_constant__ ClassArgs A,
+                                                         const MemberDev* __restrict__ members,
+                                                         const Tile* __restrict__ tiles,
+                                                         int ntiles) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    const MemberDev& m = members[tl.member];
+    const int c = tl.col0 + threadIdx.x;
+    const ConstsD& CD = A.cls[m.cls];
+    if (c < m.il) m.table[c] = zonal_row(CD.K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
+    uint32_t bit = 0;
+    if (c < m.C) {
+      switch (m.kx) {  // uniform per block
+        case 16: bit = first_process<16>(CD, m.in, m.out, c, m.C); break;
+        case 8: bit = first_process<8>(CD, m.in, m.out, c, m.C); break;
+        default: bit = first_process<7>(CD, m.in, m.out, c, m.C); break;
+      }
+    }
+    or_level_set(bit, m.S);
+  }
 }
 
 __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant__ ClassArgs A,
@@ -54,7 +71,7 @@ __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant
 
 int preload_ensemble() {
   cudaFuncAttributes a;
-  bool ok = cudaFuncGetAttributes(&a, ensemble_prepass) == cudaSuccess;
+  bool ok = cudaFuncGetAttributes(&a, ensemble_moist) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, ensemble_columns) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
 }
@@ -83,7 +100,7 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
     spd_desc_t d = classes[m.cls].desc;
     d.ix = m.ix;
     d.il = m.il;
-    const int rc = check_instance(&d, &m.in, &m.out);
+    const int rc = check_forward_instance(&d, &m.in, &m.out);
     if (rc != SPD_OK) return rc;
   }
   char* h = static_cast<char*>(plan_host);
@@ -121,9 +138,12 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   if (!classes || !plan_device || !info) return SPD_ERR_NULL;
   if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
   static bool attr_done = false;
+  static int moist_per_sm = 0;
   if (!attr_done) {
     if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_bytes<16>()) != cudaSuccess)
+                             (int)smem_bytes<16>()) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&moist_per_sm, ensemble_moist, kNT, 0) !=
+            cudaSuccess)
       return SPD_ERR_CUDA;
     attr_done = true;
   }
@@ -132,17 +152,20 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
     A.cls[i].K = make_consts(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
     A.cls[i].D = derive_constants(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
   }
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return SPD_ERR_CUDA;
   int grid = grid_blocks;
   if (grid <= 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_columns, kNT,
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_columns, kNT,
                                                       smem_bytes<16>()) != cudaSuccess)
       return SPD_ERR_CUDA;
     grid = sms * std::max(per_sm, 1);
   }
   grid = std::min(grid, info->ntiles);
+  const int grid_moist = std::min(sms * std::max(moist_per_sm, 1), info->ntiles);
   char* base = static_cast<char*>(plan_device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const MemberDev* md = reinterpret_cast<const MemberDev*>(base + 256);
@@ -150,7 +173,7 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
   if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
     return SPD_ERR_CUDA;
-  ensemble_prepass<<<grid * 2, kBlock, 0, st>>>(A, md, tl, info->ntiles);
+  ensemble_moist<<<grid_moist, kNT, 0, st>>>(A, md, tl, info->ntiles);
   if (event && cudaEventRecord(static_cast<cudaEvent_t>(event), st) != cudaSuccess)
     return SPD_ERR_CUDA;
   ensemble_columns<<<grid, kNT, smem_bytes<16>(), st>>>(A, md, tl, info->ntiles);

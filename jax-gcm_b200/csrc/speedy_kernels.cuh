@@ -33,7 +33,8 @@ __device__ __forceinline__ void or_level_set(uint32_t bit, uint32_t* S) {
   __syncthreads();  // warp_bits may be rewritten by the caller's next tile
 }
 
-// Cloud-top level bit of column c (the pre-pass work of one thread).
+// Cloud-top level bit of column c from registers (the adjoint's pre-pass; the forward takes it
+// from its first half).
 template <int KX>
 __device__ __forceinline__ uint32_t prepass_column(const Consts& K, const spd_inputs_t& in,
                                                    int c, int C) {
@@ -50,15 +51,20 @@ __device__ __forceinline__ uint32_t prepass_column(const Consts& K, const spd_in
   return 1u << min(max(icl, 0), KX - 1);
 }
 
-// The whole column c of one instance: load, physics, verify, store.  `sm` is the block's
-// shared-memory arena laid out for KX levels.
+// Where the first launch leaves its results for the second, in the call's own output planes
+// (the second launch rewrites every one of them): per level, the temperature and humidity
+// tendency accumulators in out.temperature and out.specific_humidity and qsat in out.u_wind;
+// per column, the scalars below in the first levels of out.v_wind (iptop and icltop as int
+// bit patterns).  The two precipitation fields are final after the first half and go straight
+// to their outputs.
+enum { ST_CBMF, ST_CLOUDC, ST_CLSTR, ST_IPTOP, ST_ICLTOP, kStagedScalars };
+static_assert(kStagedScalars <= 7, "the staged scalars fit the smallest level count");
+
+// Loads the column's T, q (clamped at zero under SPD_FUSE_VERIFY) and phi into shared memory;
+// returns the levels whose q was clamped.
 template <int KX>
-__device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
-                                               const spd_inputs_t& in, const spd_outputs_t& out,
-                                               uint32_t Sw, const ZonalRow* __restrict__ table,
-                                               int c, int C, int il) {
-  const Consts& K = CD.K;
-  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
+__device__ __forceinline__ uint32_t load_state(float* sm, const spd_inputs_t& in, bool verify,
+                                               int c, int C) {
   float* tp = sm + (size_t)A_T * KX * kNT + threadIdx.x;
   float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
   float* pp = sm + (size_t)A_PHI * KX * kNT + threadIdx.x;
@@ -75,6 +81,74 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
     qp[k * kNT] = q;
     pp[k * kNT] = __ldg(in.geopotential + i);
   }
+  return neg;
+}
+
+// First half of column c (humidity through clouds), in registers: stages its results and
+// returns the column's cloud-top level bit, 1 << clip(icltop, 0, kx-1).
+template <int KX>
+__device__ __forceinline__ uint32_t first_process(const ConstsD& CD, const spd_inputs_t& in,
+                                                  const spd_outputs_t& out, int c, int C) {
+  const bool verify = (CD.K.flags & SPD_FUSE_VERIFY) != 0;
+  float t[KX], q[KX], phi[KX];
+#pragma unroll
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    t[k] = __ldg(in.temperature + i);
+    const float qk = __ldg(in.specific_humidity + i);
+    q[k] = (verify && qk < 0.0f) ? 0.0f : qk;
+    phi[k] = __ldg(in.geopotential + i);
+  }
+  SurfaceIn s;
+  s.psa = __ldg(in.normalized_surface_pressure + c);
+  s.fmask = __ldg(in.fmask + c);
+  float qs[KX], dt[KX], dq[KX];
+  ColScalars o;
+  column_first<KX>(CD, t, q, phi, s, qs, dt, dq, o);
+#pragma unroll
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    out.temperature[i] = dt[k];
+    out.specific_humidity[i] = dq[k];
+    out.u_wind[i] = qs[k];
+  }
+  out.v_wind[(size_t)ST_CBMF * C + c] = o.cbmf;
+  out.v_wind[(size_t)ST_CLOUDC * C + c] = o.cloudc;
+  out.v_wind[(size_t)ST_CLSTR * C + c] = o.clstr;
+  out.v_wind[(size_t)ST_IPTOP * C + c] = __int_as_float(o.iptop);
+  out.v_wind[(size_t)ST_ICLTOP * C + c] = __int_as_float(o.icltop);
+  __stcs(out.precnv + c, o.precnv);
+  __stcs(out.precls + c, o.precls);
+  return 1u << min(max(o.icltop, 0), KX - 1);
+}
+
+// Second half of column c: reloads the state and the first half's stage, runs radiation,
+// surface fluxes and vertical diffusion, applies verify_tendencies and stores every output.
+// `sm` is the block's shared-memory arena laid out for KX levels.
+template <int KX>
+__device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
+                                               const spd_inputs_t& in, const spd_outputs_t& out,
+                                               uint32_t Sw, const ZonalRow* __restrict__ table,
+                                               int c, int C, int il) {
+  const Consts& K = CD.K;
+  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
+  const uint32_t neg = load_state<KX>(sm, in, verify, c, C);
+  float* qsp = sm + (size_t)A_QSAT * KX * kNT + threadIdx.x;
+  float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
+  float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
+#pragma unroll 4
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    dtp[k * kNT] = __ldcs(out.temperature + i);
+    dqp[k * kNT] = __ldcs(out.specific_humidity + i);
+    qsp[k * kNT] = __ldcs(out.u_wind + i);
+  }
+  ColScalars o;
+  o.cbmf = __ldcs(out.v_wind + (size_t)ST_CBMF * C + c);
+  o.cloudc = __ldcs(out.v_wind + (size_t)ST_CLOUDC * C + c);
+  o.clstr = __ldcs(out.v_wind + (size_t)ST_CLSTR * C + c);
+  o.iptop = __float_as_int(__ldcs(out.v_wind + (size_t)ST_IPTOP * C + c));
+  o.icltop = __float_as_int(__ldcs(out.v_wind + (size_t)ST_ICLTOP * C + c));
   SurfaceIn s;
   s.psa = __ldg(in.normalized_surface_pressure + c);
   s.u_low = __ldg(in.u_wind + (size_t)(KX - 1) * C + c);
@@ -89,10 +163,8 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   s.orog = __ldg(in.orog + c);
   s.phis0 = __ldg(in.phis0 + c);
   const ZonalRow z = table[c % il];
-  ColScalars o;
-  column_smem<KX>(CD, sm, s, z, Sw, o);
-  const float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
-  float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
+  column_second<KX>(CD, sm, s, z, Sw, o);
+  const float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
   // verify_tendencies (physics_interface.py:321-342) with the unclamped humidity
   if (verify) {
     const float dt = K.dt_seconds;
@@ -114,8 +186,6 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
     const float dq = dqp[k * kNT];
     __stcs(out.specific_humidity + i, qs != 1.0f ? dq * qs : dq);
   }
-  __stcs(out.precnv + c, o.precnv);
-  __stcs(out.precls + c, o.precls);
   if (out.cbmf) out.cbmf[c] = o.cbmf;
   if (out.cloudc) out.cloudc[c] = o.cloudc;
   if (out.cloudstr) out.cloudstr[c] = o.clstr;
@@ -133,15 +203,16 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   if (out.icltop) out.icltop[c] = o.icltop;
 }
 
-// Cloud-top pre-pass of one instance: the level set S (block OR, one atomic per block) and the
-// per-latitude solar table.
+// First launch over one instance: the first half of every column, the level set S (block OR,
+// one atomic per block) and the per-latitude solar table.
 template <int KX>
-__global__ void __launch_bounds__(kBlock) cloudtop_prepass(const Consts K, const spd_inputs_t in,
-                                                           uint32_t* __restrict__ S,
-                                                           ZonalRow* __restrict__ table) {
-  const int c = blockIdx.x * kBlock + threadIdx.x;
-  if (c < K.il) table[c] = zonal_row(K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
-  const uint32_t bit = (c < K.C) ? prepass_column<KX>(K, in, c, K.C) : 0u;
+__global__ void __launch_bounds__(kNT, 5) moist_kernel(const ConstsD CD, const spd_inputs_t in,
+                                                       const spd_outputs_t out,
+                                                       uint32_t* __restrict__ S,
+                                                       ZonalRow* __restrict__ table) {
+  const int c = blockIdx.x * kNT + threadIdx.x;
+  if (c < CD.K.il) table[c] = zonal_row(CD.K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
+  const uint32_t bit = (c < CD.K.C) ? first_process<KX>(CD, in, out, c, CD.K.C) : 0u;
   or_level_set(bit, S);
 }
 

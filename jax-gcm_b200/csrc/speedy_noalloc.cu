@@ -16,7 +16,8 @@
 
 namespace spd {
 // Defined in speedy_api.cu.
-int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out);
+int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
+                           const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
                  uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker);
@@ -54,7 +55,7 @@ int scratch_address(void** out) {
 extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
                                const spd_params_t* params, const spd_inputs_t* in,
                                const spd_outputs_t* out, void* stream) {
-  int rc = spd::check_instance(desc, in, out);
+  int rc = spd::check_forward_instance(desc, in, out);
   if (rc != SPD_OK) return rc;
   if (!vgrid || !params) return SPD_ERR_NULL;
   if (desc->il > SPD_NOALLOC_MAX_IL) return SPD_ERR_NOALLOC_LIMIT;

@@ -188,3 +188,13 @@ def parity_check(pkg, inst, params=None, max_flip_frac=2e-3, device="cuda", **kw
     assert summ["flip_columns"] <= max(2, max_flip_frac * summ["columns"]), summ
     assert not x64_violations(x64), x64_violations(x64)
     return rep, summ
+
+
+def fake_fields(L, base=1 << 36, spacing=1 << 28):
+    """Inputs and Outputs structs of distinct, non-overlapping, aligned fake device addresses
+    (one `spacing`-sized slot per field), for argument checks that return before any device
+    work and never dereference them."""
+    n_in = len(L.INPUT_FIELDS)
+    inp = L.Inputs(**{k: base + i * spacing for i, k in enumerate(L.INPUT_FIELDS)})
+    out = L.Outputs(**{k: base + (n_in + i) * spacing for i, k in enumerate(L.OUTPUT_FIELDS)})
+    return inp, out

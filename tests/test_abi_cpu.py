@@ -8,6 +8,8 @@ import re
 import numpy as np
 import pytest
 
+from tests.helpers import fake_fields
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -92,6 +94,26 @@ def test_argument_validation_needs_no_gpu(pkg, lib):
                      None)
     assert rc == 3
     assert lib.spd_status_string(3).decode().startswith("unsupported")
+
+
+def test_overlapping_outputs_are_rejected(pkg, lib):
+    L = pkg._lib
+    d = L.Desc(8, 16, 8, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    vg, pr = L.VGrid(), L.Params()
+    call = lambda i, o: lib.spd_fwd(C.byref(d), C.byref(vg), C.byref(pr), C.byref(i), C.byref(o),
+                                    None, 0, None)
+    inp, out = fake_fields(L)
+    assert call(inp, out) == 4  # disjoint: reaches the scratch check
+    inp, out = fake_fields(L)
+    out.temperature = inp.temperature  # in-place update
+    assert call(inp, out) == 9
+    inp, out = fake_fields(L)
+    out.cbmf = out.precls + 16
+    assert call(inp, out) == 9  # a diagnostic overlapping a required output
+    inp, out = fake_fields(L)
+    out.evap = inp.coa - 16
+    assert call(inp, out) == 9  # a diagnostic running into a latitude table
+    assert lib.spd_status_string(9).decode().startswith("an output field overlaps")
 
 
 def test_product_path_fails_loudly_without_library(pkg, monkeypatch):

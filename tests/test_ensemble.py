@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import speedy_oracle as O
-from tests.helpers import compare_fields, to_device
+from tests.helpers import compare_fields, fake_fields, to_device
 
 
 @pytest.fixture(scope="module")
@@ -17,9 +17,7 @@ def pkg():
 
 def _fake_member(L, ix, il, cls):
     m = L.Member()
-    fake = 1 << 24
-    m.inp = L.Inputs(**{k: fake for k in L.INPUT_FIELDS})
-    m.out = L.Outputs(**{k: fake for k in L.OUTPUT_FIELDS})
+    m.inp, m.out = fake_fields(L)  # never dereferenced by the plan
     m.ix, m.il, m.cls = ix, il, cls
     return m
 

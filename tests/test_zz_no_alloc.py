@@ -14,7 +14,7 @@ import importlib
 import numpy as np
 import pytest
 
-from tests.helpers import RTOL, to_device
+from tests.helpers import RTOL, fake_fields, to_device
 
 
 @pytest.fixture(scope="module")
@@ -85,9 +85,8 @@ def test_noalloc_rejects_too_many_latitudes(pkg):
     L = pkg._lib
     il = L.NOALLOC_MAX_IL + 2
     desc = L.Desc(8, 4, il, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
-    fake = 1 << 20  # aligned, never dereferenced: the call returns before touching the GPU
-    inp = L.Inputs(**{k: fake for k in L.INPUT_FIELDS})
-    outs = L.Outputs(**{k: fake for k in L.OUTPUT_FIELDS})
+    # aligned, never dereferenced: the call returns before touching the GPU
+    inp, outs = fake_fields(L)
     vg, pr = L.VGrid(), L.Params()
     rc = lib.spd_fwd_noalloc(C.byref(desc), C.byref(vg), C.byref(pr), C.byref(inp),
                              C.byref(outs), None)
