@@ -28,16 +28,16 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes (read + write) per column of the dominant kernel's launch, from one ncu capture
-# each (profiles/ensemble_columns_ragged_ensemble.md: 96.2 MB read + 48.9 MB written by one
-# ensemble_columns launch over 466,944 columns; profiles/column_kernel_k16_t425.md: 196.7 + 160.2
-# MB by column_kernel<16> over 819,200 columns).  Part of each launch's writes is still in L2 when
-# the kernel ends, so the write share reads low.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.211456e6 + 48.920064e6) / 466944,
-                          "t425": (196.67712e6 + 160.18688e6) / 819200}
+# DRAM bytes (read + write) per column of the dominant kernel's launch (the second launch,
+# ensemble_columns), from one ncu capture each (profiles/ensemble_columns_ragged_ensemble.md:
+# 179.1 MB read + 47.9 MB written over 466,944 columns; profiles/ensemble_columns_t425.md:
+# 370.4 + 157.2 MB over 819,200 columns).  Part of each launch's writes is still in L2 when the
+# kernel ends, so the write share reads low.
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": (179.072512e6 + 47.920896e6) / 466944,
+                          "t425": (370.371328e6 + 157.233664e6) / 819200}
 # Warp instructions per launch of the dominant kernel (smsp__inst_executed.sum, same captures):
 # the compute side of the roofline, against one instruction per scheduler per cycle.
-NCU_WARP_INSTRUCTIONS = {"ensemble": 142825231.0, "t425": 306628651.0}
+NCU_WARP_INSTRUCTIONS = {"ensemble": 106901715.0, "t425": 227572248.0}
 
 
 def parse_args():
@@ -158,6 +158,8 @@ def run_b200(args):
     members = workload_members(pkg, args.workload, rank)
     cols = sum(m.columns for m in members)
     bytes_step = sum(pkg.synthetic.fwd_bytes(m.kx, m.columns) for m in members)
+    bytes_first = sum(pkg.synthetic.first_half_bytes(m.kx, m.columns) for m in members)
+    bytes_second = sum(pkg.synthetic.second_half_bytes(m.kx, m.columns) for m in members)
 
     # device-resident inputs and preallocated outputs
     runs = []
@@ -214,8 +216,8 @@ def run_b200(args):
             ms = float(t.item())
         return ms
 
-    # The timed region: K steps between two events, with a marker event between the pre-pass
-    # and the column pass of every step (batched mode) so the column kernel is timed alone.
+    # The timed region: K steps between two events, with a marker event between the two
+    # launches of every step (batched mode) so that the second launch is timed alone.
     marks = [(primed_event(), primed_event(), primed_event()) for _ in range(args.steps)]
     for _ in range(args.warmup):
         step()
@@ -257,20 +259,29 @@ def run_b200(args):
                  "launches_per_step": 2 * len(runs),
                  "batched_over_plain": round(pms / ms_step, 2)}
 
-    # roofline of the dominant kernel (the column pass): the algorithmic bytes of one forward
-    # (every input read once, every output written once) over its own event-timed duration
+    # roofline of the dominant kernel (the second launch, radiation through vertical diffusion):
+    # the bytes that launch must move (its inputs and the first launch's stage read once, its
+    # outputs written once) over its own event-timed duration; the first launch and the whole
+    # step (the path's own inputs and outputs, once) beside it
     peak, peak_kind = load_peaks()
     kern_ms = col_ms if col_ms is not None else ms_step
-    achieved = bytes_step / (kern_ms / 1e3) / 1e9
+    two = col_ms is not None
+    achieved = (bytes_second if two else bytes_step) / (kern_ms / 1e3) / 1e9
     traffic = NCU_TRAFFIC_PER_COLUMN.get(args.workload)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "kernel": ("ensemble_columns" if ens is not None
-                           else "cloudtop_prepass + column_kernel (one forward per member)"),
+                "kernel": ("ensemble_columns" if two
+                           else "ensemble_moist + ensemble_columns (one forward per member)"),
                 "kernel_ms": round(kern_ms, 4),
-                "prepass_ms": (round(pre_ms, 4) if pre_ms is not None else None),
-                "algorithmic_bytes_per_launch": bytes_step,
+                "algorithmic_bytes_per_launch": bytes_second if two else bytes_step,
                 "traffic": (round(traffic * cols) if traffic else None)}
+    if two:
+        roofline["first_launch"] = {
+            "kernel": "ensemble_moist", "ms": round(pre_ms, 4),
+            "algorithmic_bytes": bytes_first,
+            "achieved_gbs": round(bytes_first / (pre_ms / 1e3) / 1e9, 1)}
+        roofline["step"] = {"path_algorithmic_bytes": bytes_step, "ms": round(ms_step, 4),
+                            "achieved_gbs": round(bytes_step / (ms_step / 1e3) / 1e9, 1)}
     # the bound that governs this kernel: instruction issue (one warp instruction per scheduler
     # per cycle), with the instruction count of the ncu capture and the SM clock sampled here
     insts = NCU_WARP_INSTRUCTIONS.get(args.workload)
@@ -381,7 +392,7 @@ def event_ms(fn, reps, warmup=3):
 
 
 def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
-    """T425 (1280x640, 16 levels): the plain drop-in call, its column kernel timed alone, and 24
+    """T425 (1280x640, 16 levels): the plain drop-in call, its two launches timed apart, and 24
     consecutive calls captured in one CUDA graph."""
     import torch
     inst = pkg.synthetic.t425_instance()
@@ -403,6 +414,7 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
         b.record()
     torch.cuda.synchronize()
     call_ms = sum(a.elapsed_time(b) for (a, m, b) in marks) / reps
+    first_ms = sum(a.elapsed_time(m) for (a, m, b) in marks) / reps
     col_ms = sum(m.elapsed_time(b) for (a, m, b) in marks) / reps
     # 24 calls in one graph
     s = torch.cuda.Stream(dev)
@@ -417,21 +429,27 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
     graph_ms = event_ms(g.replay, 5, warmup=2) / 24
     cols = inst.columns
     nbytes = pkg.synthetic.fwd_bytes(inst.kx, cols)
-    bw = nbytes / (col_ms / 1e3) / 1e9
+    b2 = pkg.synthetic.second_half_bytes(inst.kx, cols)
+    b1 = pkg.synthetic.first_half_bytes(inst.kx, cols)
+    bw = b2 / (col_ms / 1e3) / 1e9
     out_d = {"workload": "T425 1280x640, 16 levels, one instance", "columns": cols,
-             "algorithmic_bytes_per_call": nbytes,
-             "plain_call_ms": round(call_ms, 4), "column_kernel_ms": round(col_ms, 4),
+             "path_algorithmic_bytes_per_call": nbytes,
+             "plain_call_ms": round(call_ms, 4), "first_launch_ms": round(first_ms, 4),
+             "second_launch_ms": round(col_ms, 4),
              "graph_24_calls_ms_per_call": round(graph_ms, 4),
              "columns_per_s_plain": round(cols / (call_ms / 1e3), 1),
              "columns_per_s_graph": round(cols / (graph_ms / 1e3), 1),
-             "column_kernel_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
-             "column_kernel_hbm_frac": round(bw / peak, 4),
-             "column_kernel_traffic": round(NCU_TRAFFIC_PER_COLUMN["t425"] * cols)}
+             "first_launch_algorithmic_bytes": b1,
+             "first_launch_hbm_gbs": round(b1 / (first_ms / 1e3) / 1e9, 1),
+             "second_launch_algorithmic_bytes": b2,
+             "second_launch_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
+             "second_launch_hbm_frac": round(bw / peak, 4),
+             "second_launch_traffic": round(NCU_TRAFFIC_PER_COLUMN["t425"] * cols)}
     if sm_mhz:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         peak_issue = sms * 4 * sm_mhz * 1e6
         ach = NCU_WARP_INSTRUCTIONS["t425"] / (col_ms / 1e3)
-        out_d["column_kernel_issue_frac"] = round(ach / peak_issue, 4)
+        out_d["second_launch_issue_frac"] = round(ach / peak_issue, 4)
         out_d["issue_roofline_note"] = ("warp instructions per launch from ncu over one "
                                         "instruction per scheduler per cycle at the sampled "
                                         "SM clock")

@@ -127,16 +127,20 @@ typedef struct {
 size_t spd_fwd_scratch_bytes(const spd_desc_t* desc);
 
 /* SpeedyPhysics.compute_tendencies for one instance (speedy_physics.py:88-127).
- * Two launches on `stream`: a cloud-top pre-pass that forms the instance's level set
- * (shortwave_radiation.py:62-68) and the fused column kernel.  `scratch` must be 256-byte
- * aligned and at least spd_fwd_scratch_bytes(desc) long; it is initialised by the call. */
+ * Two launches on `stream`, each over every column: the first half of the column physics
+ * (humidity, convection, large-scale condensation, clouds), which also forms the instance's
+ * cloud-top level set (shortwave_radiation.py:62-68) and leaves intermediate values in the
+ * output planes; then the second half (radiation, surface fluxes, vertical diffusion), which
+ * writes every output.  They are the batched kernels below run on a one-member plan, so the
+ * results equal the batched path's bitwise.  `scratch` must be 256-byte aligned and at least
+ * spd_fwd_scratch_bytes(desc) long; it is initialised by the call. */
 int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
             const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
             size_t scratch_bytes, void* stream);
 
 /* Timing hook (no reference counterpart): spd_fwd, recording `event` (a cudaEvent_t, or NULL)
- * on `stream` between the cloud-top pre-pass and the column kernel, so that a caller can time
- * the two launches separately with events. */
+ * on `stream` between its two launches, so that a caller can time them separately with
+ * events. */
 int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
                    const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
                    size_t scratch_bytes, void* stream, void* event);
@@ -187,7 +191,7 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 /* ----------------------------------------------------------------------------------------- */
 /* Batched ragged ensemble: many instances ("members") of mixed resolution and level count,  */
 /* e.g. a forecast ensemble or a set of independent grids, in one pair of persistent launches  */
-/* (cloud-top pre-pass over every member, then the column pass over every member).  Each      */
+/* (first half of every member's columns, then the second half of every member's columns).   */
 /* member gives the same results as spd_fwd on it alone.  There is no reference counterpart   */
 /* for the batching itself; per member it replaces SpeedyPhysics.compute_tendencies           */
 /* (speedy_physics.py:88-127).                                                               */
@@ -233,7 +237,7 @@ int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 
 /* Timing hook (no reference counterpart): spd_ensemble_fwd, recording `event` (a cudaEvent_t,
- * or NULL) on `stream` between the pre-pass and the column pass. */
+ * or NULL) on `stream` between its two launches (the first and the second half). */
 int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
                             const spd_plan_info_t* info, int grid_blocks, void* stream,
                             void* event);

@@ -107,8 +107,9 @@ class Ensemble:
         return tuple(sorted((m.geometry.nodal_shape for m in self.members)))
 
     def forward(self, grid_blocks=None, marker=None):
-        """Runs every member.  ``marker`` (a torch.cuda.Event) is recorded between the pre-pass
-        and the column pass, for timing the two launches separately."""
+        """Runs every member.  ``marker`` (a torch.cuda.Event) is recorded between the two
+        launches (the first and second halves of the column physics), for timing them
+        separately."""
         lib = _lib.load()
         gb = self.grid_blocks if grid_blocks is None else grid_blocks
         stream = torch.cuda.current_stream(self.device).cuda_stream

@@ -1,34 +1,24 @@
-// speedy_api.cu -- kernels and C-ABI entry points of the plain per-instance drop-in.
+// speedy_api.cu -- C-ABI entry points of the plain per-instance drop-in.
 //
 // spd_fwd runs two launches on the caller's stream, together the fused physics of every
-// column (speedy_physics.py:88-127):
-//   1. moist_kernel: humidity, convection, large-scale condensation and clouds.  Every column
+// column (speedy_physics.py:88-127); both are the batched kernels of speedy_ensemble.cu, run
+// over a one-member plan passed by value:
+//   1. ensemble_moist: humidity, convection, large-scale condensation and clouds.  Every column
 //      forms its cloud-top level clip(icltop, 0, kx-1) and the instance ORs them into one
 //      32-bit level set S (the cross-column dependency of shortwave_radiation.py:62-68); the
 //      same launch writes the per-latitude solar table and stages the column's partial
 //      tendencies, qsat and cloud scalars in the output planes.
-//   2. column_kernel: radiation, surface fluxes and vertical diffusion, reading S and the
+//   2. ensemble_columns: radiation, surface fluxes and vertical diffusion, reading S and the
 //      stage, then verify_tendencies and every output.
 // One thread owns one column (speedy_kernels.cuh, speedy_column_smem.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "speedy_kernels.cuh"
+#include "speedy_ensemble.cuh"
 
 namespace spd {
 
 constexpr size_t kHeaderBytes = 256;  // S word, status word, padding
-
-template <int KX>
-__global__ void __launch_bounds__(kNT, 4) column_kernel(const ConstsD CD, const spd_inputs_t in,
-                                                        const spd_outputs_t out,
-                                                        const uint32_t* __restrict__ S,
-                                                        const ZonalRow* __restrict__ table) {
-  extern __shared__ float sm[];
-  const int c = blockIdx.x * kNT + threadIdx.x;
-  if (c >= CD.K.C) return;
-  column_process<KX>(CD, sm, in, out, __ldg(S), table, c, CD.K.C, CD.K.il);
-}
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
@@ -119,59 +109,38 @@ Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_
   return K;
 }
 
-template <int KX>
-static int launch_fwd(const ConstsD& CD, const spd_inputs_t& in, const spd_outputs_t& out,
-                      uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker) {
-  static bool attr_done = false;  // per template instance; idempotent, so races are harmless
-  if (!attr_done) {
-    if (cudaFuncSetAttribute(column_kernel<KX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem_bytes<KX>()) != cudaSuccess)
-      return SPD_ERR_CUDA;
-    attr_done = true;
-  }
-  const Consts& K = CD.K;
-  const int grid = (K.C + kNT - 1) / kNT;  // C = ix * il >= il covers the solar table too
-  moist_kernel<KX><<<grid, kNT, 0, st>>>(CD, in, out, S, table);
-  if (marker && cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
-  column_kernel<KX><<<grid, kNT, smem_bytes<KX>(), st>>>(CD, in, out, S, table);
-  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
-}
-
+// The forward of one instance: the batched kernels over an implicit one-member plan passed
+// by value (tile t = columns t*kNT ..), one block per tile.  The plain and the batched path
+// therefore run the same code and agree bitwise.
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
                  uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker) {
-  switch (kx) {
-    case 7: return launch_fwd<7>(CD, in, out, S, table, st, marker);
-    case 8: return launch_fwd<8>(CD, in, out, S, table, st, marker);
-    case 16: return launch_fwd<16>(CD, in, out, S, table, st, marker);
-    default: return SPD_ERR_KX;
-  }
+  if (kx != 7 && kx != 8 && kx != 16) return SPD_ERR_KX;
+  ClassArgs A;
+  A.cls[0] = CD;
+  TileSource T{};
+  T.single.in = in;
+  T.single.out = out;
+  T.single.C = CD.K.C;
+  T.single.il = CD.K.il;
+  T.single.kx = kx;
+  T.single.cls = 0;
+  T.single.S = S;
+  T.single.table = table;
+  const int ntiles = (CD.K.C + kNT - 1) / kNT;
+  return launch_forward(A, T, ntiles, kx, ntiles, ntiles, st, marker);
 }
 
 int preload_ensemble();
 int preload_adjoint();
-
-// Loads this translation unit's kernels (see spd_preload).
-static int preload_api() {
-  cudaFuncAttributes a;
-  bool ok = true;
-  ok &= cudaFuncGetAttributes(&a, column_kernel<7>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, column_kernel<8>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, column_kernel<16>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, moist_kernel<7>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, moist_kernel<8>) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, moist_kernel<16>) == cudaSuccess;
-  return ok ? SPD_OK : SPD_ERR_CUDA;
-}
 
 }  // namespace spd
 
 extern "C" {
 
 int spd_preload(void) {
-  const int a = spd::preload_api();
   const int b = spd::preload_ensemble();
   const int c = spd::preload_adjoint();
-  return (a == SPD_OK && b == SPD_OK && c == SPD_OK) ? SPD_OK : SPD_ERR_CUDA;
+  return (b == SPD_OK && c == SPD_OK) ? SPD_OK : SPD_ERR_CUDA;
 }
 
 

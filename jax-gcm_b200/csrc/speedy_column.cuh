@@ -114,7 +114,7 @@ __device__ __forceinline__ ZonalRow zonal_row(float tyear, float sia, float coa)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Stages shared by the cloud-top pre-pass and the full column.
+// Stages of the adjoint's cloud-top pre-pass (the level set S from registers).
 // ---------------------------------------------------------------------------------------------
 
 // diagnose_convection (convection.py:15-97).  Returns iptop; qdif through the reference.

@@ -8,7 +8,8 @@
 // first half of every column on all tiles (each member's level set, solar table and staged
 // values, as in spd_fwd's first launch); launch 2 runs the second half on all tiles, reading
 // each member's level set.  Both launches are persistent: gridDim blocks stride over the tile
-// list.
+// list.  The plain per-instance forward (spd_fwd) runs the same two kernels over a one-member
+// plan given by value, so that the two paths agree bitwise.
 // Constants shared by a class of members (kx, date, switches, vertical grid, parameters) travel
 // by value in the kernel parameters.
 #include <cuda_runtime.h>
@@ -27,13 +28,12 @@ int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
 __global__ void __launch_bounds__(kNT, 5) ensemble_moist(const __grid_constant__ ClassArgs A,
-                                                         const MemberDev* __restrict__ members,
-                                                         const Tile* __restrict__ tiles,
+                                                         const __grid_constant__ TileSource T,
                                                          int ntiles) {
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    const MemberDev& m = members[tl.member];
-    const int c = tl.col0 + threadIdx.x;
+    int col0;
+    const MemberDev m = tile_member(T, t, col0);
+    const int c = col0 + threadIdx.x;
     const ConstsD& CD = A.cls[m.cls];
     if (c < m.il) m.table[c] = zonal_row(CD.K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
     uint32_t bit = 0;
@@ -49,14 +49,13 @@ __global__ void __launch_bounds__(kNT, 5) ensemble_moist(const __grid_constant__
 }
 
 __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant__ ClassArgs A,
-                                                           const MemberDev* __restrict__ members,
-                                                           const Tile* __restrict__ tiles,
+                                                           const __grid_constant__ TileSource T,
                                                            int ntiles) {
   extern __shared__ float sm[];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = tiles[t];
-    const MemberDev& m = members[tl.member];
-    const int c = tl.col0 + threadIdx.x;
+    int col0;
+    const MemberDev m = tile_member(T, t, col0);
+    const int c = col0 + threadIdx.x;
     if (c < m.C) {
       const ConstsD& CD = A.cls[m.cls];
       const uint32_t Sw = *m.S;
@@ -67,6 +66,23 @@ __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant
       }
     }
   }
+}
+
+static size_t arena_bytes(int kx) { return (size_t)kNumArrays * kx * kNT * sizeof(float); }
+
+int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_layout,
+                   int grid_moist, int grid_cols, cudaStream_t st, cudaEvent_t marker) {
+  static bool attr_done = false;  // idempotent, so races are harmless
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<16>()) != cudaSuccess)
+      return SPD_ERR_CUDA;
+    attr_done = true;
+  }
+  ensemble_moist<<<grid_moist, kNT, 0, st>>>(A, T, ntiles);
+  if (marker && cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
+  ensemble_columns<<<grid_cols, kNT, arena_bytes(kx_layout), st>>>(A, T, ntiles);
+  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
 int preload_ensemble() {
@@ -137,47 +153,43 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   using namespace spd;
   if (!classes || !plan_device || !info) return SPD_ERR_NULL;
   if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
-  static bool attr_done = false;
-  static int moist_per_sm = 0;
-  if (!attr_done) {
+  static int moist_per_sm = 0, cols_per_sm = 0;  // idempotent, so races are harmless
+  if (moist_per_sm == 0) {
+    int m = 0, c = 0;
     if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes<16>()) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&moist_per_sm, ensemble_moist, kNT, 0) !=
-            cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, ensemble_moist, kNT, 0) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, ensemble_columns, kNT,
+                                                      smem_bytes<16>()) != cudaSuccess)
       return SPD_ERR_CUDA;
-    attr_done = true;
+    cols_per_sm = std::max(c, 1);
+    moist_per_sm = std::max(m, 1);
   }
   ClassArgs A;
+  int kx_layout = 0;
   for (int i = 0; i < nclasses; ++i) {
     A.cls[i].K = make_consts(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
     A.cls[i].D = derive_constants(&classes[i].desc, &classes[i].vgrid, &classes[i].params);
+    kx_layout = std::max(kx_layout, classes[i].desc.kx);
   }
+  if (kx_layout != 7 && kx_layout != 8 && kx_layout != 16) return SPD_ERR_KX;
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return SPD_ERR_CUDA;
-  int grid = grid_blocks;
-  if (grid <= 0) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_columns, kNT,
-                                                      smem_bytes<16>()) != cudaSuccess)
-      return SPD_ERR_CUDA;
-    grid = sms * std::max(per_sm, 1);
-  }
-  grid = std::min(grid, info->ntiles);
-  const int grid_moist = std::min(sms * std::max(moist_per_sm, 1), info->ntiles);
+  const int grid = std::min(grid_blocks > 0 ? grid_blocks : sms * cols_per_sm, info->ntiles);
+  const int grid_moist = std::min(sms * moist_per_sm, info->ntiles);
   char* base = static_cast<char*>(plan_device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const MemberDev* md = reinterpret_cast<const MemberDev*>(base + 256);
-  const size_t tiles_off = 256 + align256((size_t)info->nmembers * sizeof(MemberDev));
-  const Tile* tl = reinterpret_cast<const Tile*>(base + tiles_off);
+  TileSource T{};
+  T.members = reinterpret_cast<const MemberDev*>(base + 256);
+  T.tiles = reinterpret_cast<const Tile*>(
+      base + 256 + align256((size_t)info->nmembers * sizeof(MemberDev)));
   if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
     return SPD_ERR_CUDA;
-  ensemble_moist<<<grid_moist, kNT, 0, st>>>(A, md, tl, info->ntiles);
-  if (event && cudaEventRecord(static_cast<cudaEvent_t>(event), st) != cudaSuccess)
-    return SPD_ERR_CUDA;
-  ensemble_columns<<<grid, kNT, smem_bytes<16>(), st>>>(A, md, tl, info->ntiles);
-  return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+  return launch_forward(A, T, info->ntiles, kx_layout, grid_moist, grid, st,
+                        static_cast<cudaEvent_t>(event));
 }
 
 }  // extern "C"

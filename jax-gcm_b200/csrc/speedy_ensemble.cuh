@@ -1,6 +1,7 @@
 // speedy_ensemble.cuh -- what the batched forward and the batched adjoint share: the tile
-// list over ragged members, the per-class constants passed by value, and the cloud-top
-// pre-pass over all tiles (each member's level set and per-latitude solar table).
+// list over ragged members, the per-class constants passed by value, and the adjoint's
+// cloud-top pre-pass over all tiles (each member's level set and per-latitude solar table;
+// the forward forms both in its first launch).
 #pragma once
 
 #include <algorithm>
@@ -25,6 +26,34 @@ struct ClassArgs {
 struct Tile {
   int member, col0;
 };
+
+// Where a forward launch takes its tiles from: a plan's member table and tile list, or (when
+// `members` is null) the one member given by value, whose tile t covers columns
+// t*kNT .. t*kNT + kNT - 1.  Passed by value to the kernels.
+struct TileSource {
+  const MemberDev* members;
+  const Tile* tiles;
+  MemberDev single;
+};
+
+// The member of tile t, copied: the kernels read its field pointers from the copy, which no
+// store to an output field can alias (a reference into the plan would make the compiler reload
+// the pointers after every store).
+__device__ __forceinline__ MemberDev tile_member(const TileSource& T, int t, int& col0) {
+  if (T.members == nullptr) {
+    col0 = t * kNT;
+    return T.single;
+  }
+  const Tile tl = T.tiles[t];
+  col0 = tl.col0;
+  return T.members[tl.member];
+}
+
+// Both launches of the forward (speedy_ensemble.cu): grid_moist and grid_cols blocks stride
+// over the ntiles tiles; kx_layout is the largest level count among them (it sizes the second
+// launch's shared-memory arena).
+int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_layout,
+                   int grid_moist, int grid_cols, cudaStream_t st, cudaEvent_t marker);
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 

@@ -203,17 +203,4 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   if (out.icltop) out.icltop[c] = o.icltop;
 }
 
-// First launch over one instance: the first half of every column, the level set S (block OR,
-// one atomic per block) and the per-latitude solar table.
-template <int KX>
-__global__ void __launch_bounds__(kNT, 5) moist_kernel(const ConstsD CD, const spd_inputs_t in,
-                                                       const spd_outputs_t out,
-                                                       uint32_t* __restrict__ S,
-                                                       ZonalRow* __restrict__ table) {
-  const int c = blockIdx.x * kNT + threadIdx.x;
-  if (c < CD.K.il) table[c] = zonal_row(CD.K.tyear, __ldg(in.sia + c), __ldg(in.coa + c));
-  const uint32_t bit = (c < CD.K.C) ? first_process<KX>(CD, in, out, c, CD.K.C) : 0u;
-  or_level_set(bit, S);
-}
-
 }  // namespace spd

@@ -70,7 +70,7 @@ extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
   spd::ZonalRow* table =
       reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + kNoallocHeader);
   // The array keeps the previous call's contents: the level-set and status words must start
-  // at zero; the solar table is fully rewritten by the pre-pass.
+  // at zero; the solar table is fully rewritten by the first launch.
   if (cudaMemsetAsync(S, 0, kNoallocHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
   return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st, nullptr);
 }

@@ -464,8 +464,9 @@ class SpeedyPhysics(Physics):
     def compute_tendencies(self, state: PhysicsState, forcing: ForcingData, geometry: Geometry,
                            date: DateData, out: Optional[dict] = None, marker=None):
         """Tendencies and PhysicsData for ``state``.  ``out`` may give preallocated output
-        tensors; ``marker`` (a torch.cuda.Event) is recorded between the cloud-top pre-pass and
-        the column kernel, for timing the two launches separately."""
+        tensors (they must not overlap the inputs); ``marker`` (a torch.cuda.Event) is recorded
+        between the two launches (the first and second halves of the column physics), for
+        timing them separately."""
         lib = _lib.load()
         kx, ix, il = geometry.nodal_shape
         t = state.temperature

@@ -208,3 +208,17 @@ def fwd_bytes(kx, columns):
     level, psa, six forcing fields and three geometry fields read; four tendency planes and two
     precipitation fields written."""
     return 4 * (7 * kx + 14) * columns
+
+
+def first_half_bytes(kx, columns):
+    """Bytes the forward's first launch must move: T, q, phi at every level, psa and fmask read;
+    the staged temperature and humidity accumulators and qsat at every level, five staged
+    scalars and the two precipitation fields written."""
+    return 4 * (6 * kx + 9) * columns
+
+
+def second_half_bytes(kx, columns):
+    """Bytes the forward's second launch must move: T, q, phi and the three staged level fields
+    at every level, the five staged scalars, psa, the lowest u and v, six forcing and three
+    geometry fields read; the four tendency planes written."""
+    return 4 * (10 * kx + 17) * columns

@@ -1,7 +1,8 @@
 """The 48-step column rollout and its checkpointed adjoint on the GPU (jax-gcm_b200/rollout.py):
 
-* checkpoints every 8 steps give bitwise the gradient of storing every state (the recomputed
-  forward is deterministic);
+* checkpoints every 8 steps give bitwise the state gradient of storing every state (the
+  recomputed forward is deterministic), and the parameter gradient up to the order of its
+  atomic sums;
 * on single-column instances (whose cloud-top level set is the column's own), the float32 GPU
   rollout's gradients agree with the float64 host rollout (tests/host/host_column.cpp)
   normwise within 1e-4, state and parameters alike, after 48 steps of float32 against float64
@@ -47,7 +48,9 @@ def test_checkpointed_equals_stored():
     for k in ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential",
               "normalized_surface_pressure"):
         assert torch.equal(getattr(g8, k), getattr(g1, k)), k
-    assert torch.allclose(p8, p1, rtol=1e-5, atol=0)
+    # the parameter gradient sums every column's contribution with atomics (order not fixed),
+    # and some of its entries cancel: compare normwise
+    assert float((p8 - p1).abs().max()) <= 1e-5 * float(p1.abs().max())
 
 
 def one_column(inst, i, j):
