@@ -231,8 +231,12 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
                       int nmembers, void* plan_host, void* plan_device, size_t plan_bytes,
                       spd_plan_info_t* info);
 
-/* Runs every member.  grid_blocks = 0 picks SMs x resident blocks; otherwise the persistent
- * grid size (the autotuner's knob). */
+/* Runs every member.  grid_blocks = 0 picks SMs x resident blocks for both launches (each
+ * block strides over the tile list: the fastest form on an otherwise idle GPU); a positive
+ * value sets the second launch's persistent grid (the autotuner's knob); SPD_GRID_PER_TILE
+ * launches one block per tile for both launches, which shares the GPU better with concurrent
+ * kernels (a late-starting persistent block still owns its whole stride of tiles). */
+#define SPD_GRID_PER_TILE (-1)
 int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device,
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 

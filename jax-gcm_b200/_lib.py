@@ -109,6 +109,7 @@ STATUS = {0: "ok", 1: "null pointer", 2: "bad shape", 3: "unsupported kx", 4: "b
           8: "il above the no-allocation entry point's limit",
           9: "an output field overlaps an input or another output"}
 NOALLOC_MAX_IL = 2048
+GRID_PER_TILE = -1  # SPD_GRID_PER_TILE
 
 _lib = None
 _lock = threading.Lock()

@@ -153,6 +153,7 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   using namespace spd;
   if (!classes || !plan_device || !info) return SPD_ERR_NULL;
   if (nclasses <= 0 || nclasses > SPD_MAX_CLASSES || info->ntiles <= 0) return SPD_ERR_SHAPE;
+  if (grid_blocks < 0 && grid_blocks != SPD_GRID_PER_TILE) return SPD_ERR_SHAPE;
   static int moist_per_sm = 0, cols_per_sm = 0;  // idempotent, so races are harmless
   if (moist_per_sm == 0) {
     int m = 0, c = 0;
@@ -178,8 +179,11 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return SPD_ERR_CUDA;
-  const int grid = std::min(grid_blocks > 0 ? grid_blocks : sms * cols_per_sm, info->ntiles);
-  const int grid_moist = std::min(sms * moist_per_sm, info->ntiles);
+  const bool per_tile = grid_blocks == SPD_GRID_PER_TILE;
+  const int grid = per_tile ? info->ntiles
+                            : std::min(grid_blocks > 0 ? grid_blocks : sms * cols_per_sm,
+                                       info->ntiles);
+  const int grid_moist = per_tile ? info->ntiles : std::min(sms * moist_per_sm, info->ntiles);
   char* base = static_cast<char*>(plan_device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   TileSource T{};

@@ -121,6 +121,10 @@ def test_ensemble_graph_replay_and_autotune(pkg):
     insts, members, plain = _members(pkg, "cuda")
     ens = pkg.Ensemble(members, plain[0][3])
     ref = [{k: v.clone() for k, v in o.items()} for o in ens.forward()]
+    # one block per tile instead of persistent grids: the same columns, bitwise
+    for o, r in zip(ens.forward(grid_blocks=pkg._lib.GRID_PER_TILE), ref):
+        for k in r:
+            assert torch.equal(o[k], r[k]), k
     gb = ens.autotune(reps=2)
     assert gb >= 0
     for o in ens.forward():
