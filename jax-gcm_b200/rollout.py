@@ -60,6 +60,22 @@ def rollout(physics, state, forcing, geometry, date, nsteps=48, dt=1800.0):
     return x
 
 
+def rollout_with_precipitation(physics, state, forcing, geometry, date, nsteps=48,
+                               dt=1800.0):
+    """``rollout`` that also returns, per column, the precipitation (convective plus
+    large-scale, as PhysicsData reports them) averaged over the steps."""
+    ph = _physics(physics, dt)
+    x = state
+    acc = torch.zeros_like(state.normalized_surface_pressure)
+    for n in range(nsteps):
+        tend, data = ph.compute_tendencies(x, forcing, geometry, _date(date, n))
+        acc += data.convection.precnv + data.condensation.precls
+        new = {k: getattr(x, k) + dt * getattr(tend, k) for k in EVOLVED}
+        x = PhysicsState(new["u_wind"], new["v_wind"], new["temperature"],
+                         new["specific_humidity"], x.geopotential, x.normalized_surface_pressure)
+    return x, acc / nsteps
+
+
 def checkpointed_reverse(step_fn, step_vjp_fn, x0, xbar_final, nsteps, checkpoint_every):
     """Reverse pass of x_{n+1} = step_fn(x_n, n) with checkpoints.
 
