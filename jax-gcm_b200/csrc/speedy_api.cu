@@ -127,7 +127,7 @@ int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_ou
   T.single.S = S;
   T.single.table = table;
   const int ntiles = (CD.K.C + kNT - 1) / kNT;
-  return launch_forward(A, T, ntiles, kx, ntiles, ntiles, st, marker);
+  return launch_forward(A, T, ntiles, kx, SPD_GRID_PER_TILE, st, marker);
 }
 
 int preload_ensemble();

@@ -49,11 +49,23 @@ __device__ __forceinline__ MemberDev tile_member(const TileSource& T, int t, int
   return T.members[tl.member];
 }
 
-// Both launches of the forward (speedy_ensemble.cu): grid_moist and grid_cols blocks stride
-// over the ntiles tiles; kx_layout is the largest level count among them (it sizes the second
-// launch's shared-memory arena).
+// Prefetches into L2 the `nrows` rows of a full tile (row(r): the first float of row r, 128
+// consecutive floats), one prefetch per 128-byte line, spread over the block's threads.
+template <class RowFn>
+__device__ __forceinline__ void prefetch_tile_rows(int nrows, RowFn row) {
+  static_assert(kNT == 128, "a tile row is four 128-byte lines");
+  for (int i = threadIdx.x; i < nrows * 4; i += kNT) {
+    const float* p = row(i >> 2) + (i & 3) * 32;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
+// Both launches of the forward (speedy_ensemble.cu) over the ntiles tiles.  grid_blocks: 0 =
+// persistent grids of SMs x resident blocks; > 0 = the second launch's persistent grid;
+// SPD_GRID_PER_TILE = one block per tile.  kx_layout is the largest level count among the
+// tiles (it sizes the second launch's shared-memory arena).
 int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_layout,
-                   int grid_moist, int grid_cols, cudaStream_t st, cudaEvent_t marker);
+                   int grid_blocks, cudaStream_t st, cudaEvent_t marker);
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
