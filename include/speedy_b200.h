@@ -53,7 +53,12 @@ enum spd_flags {
   SPD_LSCASYM = 1u << 1,      /* SurfaceFluxParameters.lscasym (params.py:180) */
   SPD_LSKINEB = 1u << 2,      /* SurfaceFluxParameters.lskineb (params.py:181) */
   SPD_INCREASE_CO2 = 1u << 3, /* ForcingParameters.increase_co2 (params.py:34) */
-  SPD_FUSE_VERIFY = 1u << 4   /* apply verify_state before and verify_tendencies after */
+  SPD_FUSE_VERIFY = 1u << 4,  /* apply verify_state before and verify_tendencies after */
+  SPD_OROGRAPHIC = 1u << 5    /* orographic correction as the last term (orographic_correction.py
+                                 :177-247; commented out of the reference's term list at
+                                 speedy_physics.py:65,79).  Its tendency divides by
+                                 spd_desc_t.dt_seconds, which must then equal
+                                 DateData.dt_seconds. */
 };
 
 /* One grid instance: shape, switches and DateData (jcm/date.py:9-14). */

@@ -19,6 +19,7 @@ SPD_LSCASYM = 1 << 1
 SPD_LSKINEB = 1 << 2
 SPD_INCREASE_CO2 = 1 << 3
 SPD_FUSE_VERIFY = 1 << 4
+SPD_OROGRAPHIC = 1 << 5
 
 
 class Desc(C.Structure):

@@ -111,7 +111,8 @@ def _tendencies_op(u: torch.Tensor, v: torch.Tensor, t: torch.Tensor, q: torch.T
         kw = {f"{g}__{n}": float(x) for (g, n), x in zip(DIFF_PARAMS, vals)}
         phys = SpeedyPhysics(physics.parameters.with_values(**kw), fuse_verify=physics.fuse_verify,
                              time_step=physics.time_step, q_tend_scale=physics.q_tend_scale,
-                             diagnostics=False)
+                             diagnostics=False,
+                             orographic_correction=physics.orographic_correction)
     st = PhysicsState(u.contiguous(), v.contiguous(), t.contiguous(), q.contiguous(),
                       phi.contiguous(), psa.contiguous())
     tend, _ = phys.compute_tendencies(st, forcing, geometry, date)
@@ -138,7 +139,8 @@ def _backward(ctx, gu, gv, gt, gq):
         kw = {f"{g}__{n}": float(x) for (g, n), x in zip(DIFF_PARAMS, vals)}
         phys = SpeedyPhysics(physics.parameters.with_values(**kw), fuse_verify=physics.fuse_verify,
                              time_step=physics.time_step, q_tend_scale=physics.q_tend_scale,
-                             diagnostics=False)
+                             diagnostics=False,
+                             orographic_correction=physics.orographic_correction)
     z = lambda ref: torch.zeros_like(ref)
     cot = PhysicsTendency(gu if gu is not None else z(u), gv if gv is not None else z(v),
                           gt if gt is not None else z(t), gq if gq is not None else z(q))

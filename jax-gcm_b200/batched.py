@@ -36,12 +36,14 @@ class Ensemble:
     """
 
     def __init__(self, members: List[Member], date, parameters: Optional[Parameters] = None,
-                 fuse_verify=False, time_step=None, q_tend_scale=1.0):
+                 fuse_verify=False, time_step=None, q_tend_scale=1.0,
+                 orographic_correction=False):
         lib = _lib.load()
         self.members = members
         self.date = date
         self.phys = SpeedyPhysics(parameters, fuse_verify=fuse_verify, time_step=time_step,
-                                  q_tend_scale=q_tend_scale, diagnostics=False)
+                                  q_tend_scale=q_tend_scale, diagnostics=False,
+                                  orographic_correction=orographic_correction)
         dev = members[0].state.temperature.device
         self.device = dev
         _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())

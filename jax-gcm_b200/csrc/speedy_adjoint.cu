@@ -31,6 +31,7 @@ struct VjpArgs {
   uint32_t flags;
   int model_step, C, il;
   float ablco2, dt_seconds, q_tend_scale;
+  float qcorv[SPD_MAX_KX], gamlat, pexp;  // orographic correction (SPD_OROGRAPHIC)
 };
 
 // One column's VJP: loads, the reverse pass, stores; adds the parameter gradients to pacc.
@@ -73,7 +74,8 @@ __device__ __forceinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t&
   xi.stratz = z.stratz; xi.sqrt_coa = z.sqrt_coa;
   spdvjp::Bar<KX, float> b;
   spdvjp::column_vjp<KX, float>(x, g, A.ablco2, A.dt_seconds, A.q_tend_scale, xi, ct_t, ct_q,
-                                __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b);
+                                __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b, A.qcorv,
+                                A.gamlat, A.pexp);
 #pragma unroll 1
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
@@ -218,6 +220,9 @@ static VjpArgs make_vjp_args(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
   A.ablco2 = D.ablco2;
   A.dt_seconds = desc->dt_seconds;
   A.q_tend_scale = desc->q_tend_scale;
+  for (int k = 0; k < SPD_MAX_KX; ++k) A.qcorv[k] = D.qcorv[k];
+  A.gamlat = D.gamlat;
+  A.pexp = D.pexp;
   return A;
 }
 

@@ -34,6 +34,9 @@ struct Derived {
   float ablco2;               // physics/speedy/forcing.py:136
   float rgas288_sigl;         // rgas*288*sigl[kx-1]                   (surface_flux.py:111)
   float rrcl, rgse;           // shortwave_radiation.py:348, :387
+  float tcorv[SPD_MAX_KX];    // orographic temperature profile        (orographic_correction.py:18-55)
+  float qcorv[SPD_MAX_KX];    // orographic humidity profile           (orographic_correction.py:58-93)
+  float gamlat, pexp;         // orographic_correction.py:110, :151
 };
 
 // Host evaluation (plain IEEE float32 arithmetic, no contraction on the host target).
@@ -96,6 +99,19 @@ inline Derived derive_constants(const spd_desc_t* d, const spd_vgrid_t* vg,
   D.rgas288_sigl = (float)(2.0 / 7.0 * 1004.0 * 288.0) * vg->sigl[kx - 1];
   D.rrcl = 1.0f / (p->rhcl2 - p->rhcl1);
   D.rgse = 1.0f / (p->gse_s1 - p->gse_s0);
+  // orographic correction (orographic_correction.py): the reference evaluates these in float32
+  // from double constants (rgas = 2/7 * 1004, gamma = 6, g = 9.81, hscale / hshum = 3)
+  {
+    const double rgas = 2.0 / 7.0 * 1004.0, gamma = 6.0, grav = 9.81;
+    const float rgam = (float)(rgas * gamma / (1000.0 * grav));
+    const float qexp = (float)(7.5 / 2.5);
+    for (int k = 0; k < kx; ++k) {
+      D.tcorv[k] = (k == 0) ? 0.0f : powf(vg->fsg[k], rgam);
+      D.qcorv[k] = (k < 2) ? 0.0f : powf(vg->fsg[k], qexp);
+    }
+    D.gamlat = (float)(gamma / (1000.0 * grav));
+    D.pexp = (float)(1000.0 * grav / (rgas * gamma));
+  }
   return D;
 }
 

@@ -122,6 +122,23 @@ __device__ __forceinline__ uint32_t first_process(const ConstsD& CD, const spd_i
   return 1u << min(max(o.icltop, 0), KX - 1);
 }
 
+// Horizontal part of the orographic correction of one column (orographic_correction.py:96-174):
+// tcorh = gamlat phis0 and qcorh = refrh1 (qsat(tref) - qsat(tsfc, psfc)) with the land/sea
+// surface temperature tsfc, tref = tsfc + tcorh and psfc = (tsfc / tref)^pexp.  The reference's
+// get_qsat at sig <= 0 divides by the first element of a pressure field of ones
+// (humidity.py:100-101), i.e. by 1 - 0.378 e.
+__device__ __forceinline__ void orographic_horizontal(const Derived& D, float phis0, float fmask,
+                                                      float stl, float sst, float& tcorh,
+                                                      float& qcorh) {
+  tcorh = D.gamlat * phis0;
+  const float tsfc = fmask * stl + (1.0f - fmask) * sst;
+  const float tref = tsfc + tcorh;
+  const float psfc = powf(tsfc / tref, D.pexp);
+  const float qref = qsat_of(tref, 1.0f, 1.0f);
+  const float qsfc = qsat_of(tsfc, psfc, 1.0f);
+  qcorh = 0.7f * (qref - qsfc);  // refrh1 (physical_constants.py:27)
+}
+
 // Second half of column c: reloads the state and the first half's stage, runs radiation,
 // surface fluxes and vertical diffusion, applies verify_tendencies and stores every output.
 // `sm` is the block's shared-memory arena laid out for KX levels.
@@ -164,6 +181,16 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   s.phis0 = __ldg(in.phis0 + c);
   const ZonalRow z = table[c % il];
   column_second<KX>(CD, sm, s, z, Sw, o);
+  if (K.flags & SPD_OROGRAPHIC) {  // the last term (get_orographic_correction_tendencies)
+    float tcorh, qcorh;
+    orographic_horizontal(CD.D, s.phis0, s.fmask, s.stl, s.sst, tcorh, qcorh);
+    const float dts = K.dt_seconds;
+#pragma unroll 4
+    for (int k = 0; k < KX; ++k) {
+      dtp[k * kNT] = dtp[k * kNT] + (tcorh * CD.D.tcorv[k]) / dts;
+      dqp[k * kNT] = dqp[k * kNT] + (qcorh * CD.D.qcorv[k]) / dts;
+    }
+  }
   const float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
   // verify_tendencies (physics_interface.py:321-342) with the unclamped humidity
   if (verify) {

@@ -31,6 +31,8 @@ using spdgen::DiffParams;
 
 SPD_HD float fexp(float x) { return expf(x); }
 SPD_HD double fexp(double x) { return exp(x); }
+SPD_HD float fpow(float x, float y) { return powf(x, y); }
+SPD_HD double fpow(double x, double y) { return pow(x, y); }
 SPD_HD float fsqrt(float x) { return sqrtf(x); }
 SPD_HD double fsqrt(double x) { return sqrt(x); }
 SPD_HD bool fnan(float x) { return x != x; }
@@ -62,6 +64,21 @@ SPD_HD F qsat_d(F ta, F ps, F sig, F& d_t, F& d_p) {
   d_t = (F(622.0) / D + (q / D) * F(0.378)) * de;
   d_p = -(q / D) * sig;
   return q;
+}
+
+// qcorh of the orographic correction (orographic_correction.py:117-174; see the forward's
+// orographic_horizontal).  Needed by the adjoint only to select the levels verify_tendencies
+// limits: the correction depends on no differentiated input.
+template <class F>
+SPD_HD F orographic_qcorh(F phis0, F fmask, F stl, F sst, F gamlat, F pexp) {
+  const F tcorh = gamlat * phis0;
+  const F tsfc = fmask * stl + (F(1) - fmask) * sst;
+  const F tref = tsfc + tcorh;
+  const F psfc = fpow(tsfc / tref, pexp);
+  F d1, d2;
+  const F qref = qsat_d(tref, F(1), F(1), d1, d2);
+  const F qsfc = qsat_d(tsfc, psfc, F(1), d1, d2);
+  return F(0.7) * (qref - qsfc);
 }
 
 // radset (longwave_radiation.py): band fractions of the blackbody flux and their derivative
@@ -1664,12 +1681,15 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
 // in.q holds the humidity as given (before verify_state).  ct_* are the cotangents of the four
 // tendency outputs (after verify_tendencies and the humidity scale, when those are fused);
 // ct_u/ct_v are the cotangents of the lowest-level wind tendencies.  On return b holds the
-// gradients: b.q with respect to the humidity as given.
+// gradients: b.q with respect to the humidity as given.  With SPD_OROGRAPHIC and the fused
+// verify, qcorv (the orographic humidity profile) and gamlat, pexp give the correction's
+// humidity tendency, which takes part in verify_tendencies' choice of limited levels.
 // ---------------------------------------------------------------------------------------------
 template <int KX, class F>
 SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seconds,
                        F q_tend_scale, const ColumnIn<F, F>& in, const F* ct_t, const F* ct_q,
-                       F ct_u, F ct_v, Bar<KX, F>& b) {
+                       F ct_u, F ct_v, Bar<KX, F>& b, const float* qcorv = nullptr,
+                       float gamlat = 0.0f, float pexp = 0.0f) {
   const spd_params_t& p = *x.p;
   const bool verify = (x.flags & SPD_FUSE_VERIFY) != 0;
   Col<KX, F> c;
@@ -1729,6 +1749,11 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
     F du, dv;
     surface_tend<KX, F>(x, sf, dt, dq, du, dv);
     vdiff(x, c, dt, dq);
+    if (qcorv && (x.flags & SPD_OROGRAPHIC)) {  // the last term's humidity tendency
+      const F qcorh = orographic_qcorh(in.phis0, in.fmask, in.stl, in.sst, F(gamlat), F(pexp));
+      SPD_ROLL
+      for (int k = 0; k < KX; ++k) dq[k] = dq[k] + (qcorh * F(qcorv[k])) / dt_seconds;
+    }
   }
   SPD_ROLL
   for (int k = 0; k < KX; ++k) {

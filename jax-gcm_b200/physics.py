@@ -427,12 +427,17 @@ class SpeedyPhysics(Physics):
     ``time_step`` (default: ``date.dt_seconds``).  ``q_tend_scale`` multiplies the humidity
     tendency last (for the g/kg/s -> model-units conversion of
     physics_tendency_to_dynamics_tendency, physics_interface.py:286).
+    ``orographic_correction=True`` appends the orographic correction as the last term
+    (orographic_correction.py:177-247), which the reference's term list carries commented out
+    (speedy_physics.py:65,79).
     """
 
     def __init__(self, parameters: Optional[Parameters] = None, checkpoint_terms=True,
-                 fuse_verify=False, time_step=None, q_tend_scale=1.0, diagnostics=True):
+                 fuse_verify=False, time_step=None, q_tend_scale=1.0, diagnostics=True,
+                 orographic_correction=False):
         self.parameters = parameters or Parameters.default()
         self.fuse_verify = fuse_verify
+        self.orographic_correction = orographic_correction
         self.time_step = time_step
         self.q_tend_scale = q_tend_scale
         self.diagnostics = diagnostics
@@ -446,6 +451,12 @@ class SpeedyPhysics(Physics):
             flags |= _lib.SPD_LFLUXLAND
         if self.fuse_verify:
             flags |= _lib.SPD_FUSE_VERIFY
+        if self.orographic_correction:
+            # the term divides by the date's step (orographic_correction.py:236-238), the
+            # kernel by the one step it is given
+            if self.time_step is not None and float(self.time_step) != float(date.dt_seconds):
+                raise ValueError("orographic_correction needs time_step == date.dt_seconds")
+            flags |= _lib.SPD_OROGRAPHIC
         dt = date.dt_seconds if self.time_step is None else self.time_step
         return _lib.Desc(kx, ix, il, flags, float(np.float32(date.tyear)), int(date.model_year),
                          int(date.model_step), int(self.parameters.forcing.co2_year_ref),
@@ -524,7 +535,8 @@ def get_physical_tendencies_columns(state, physics, forcing, geometry, date, tim
     around it (dinosaur) stay with the caller."""
     phys = physics if physics.fuse_verify else SpeedyPhysics(
         physics.parameters, fuse_verify=True, time_step=time_step,
-        q_tend_scale=physics.q_tend_scale, diagnostics=physics.diagnostics)
+        q_tend_scale=physics.q_tend_scale, diagnostics=physics.diagnostics,
+        orographic_correction=physics.orographic_correction)
     phys.time_step = time_step
     return phys.compute_tendencies(state, forcing, geometry, date)
 

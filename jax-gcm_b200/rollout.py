@@ -35,7 +35,9 @@ EVOLVED = ("u_wind", "v_wind", "temperature", "specific_humidity")
 
 def _physics(physics: Optional[SpeedyPhysics], dt: float) -> SpeedyPhysics:
     p = physics.parameters if physics is not None else None
-    return SpeedyPhysics(p, fuse_verify=True, time_step=dt, diagnostics=False)
+    oro = physics.orographic_correction if physics is not None else False
+    return SpeedyPhysics(p, fuse_verify=True, time_step=dt, diagnostics=False,
+                         orographic_correction=oro)
 
 
 def _date(date, n):

@@ -1067,6 +1067,68 @@ TERMS = [set_physics_flags, set_forcing, spec_hum_to_rel_hum, get_convection_ten
          get_upward_longwave_rad_fluxes, get_vertical_diffusion_tend]
 
 
+# ---------------------------------------------------------------------------------------------
+# orographic_correction.py (the optional last term; commented out of the reference's term list
+# at speedy_physics.py:65,79)
+# ---------------------------------------------------------------------------------------------
+GAMMA = 6.0     # physical_constants.py:24, reference lapse rate (K/km)
+HSCALE = 7.5    # physical_constants.py:25
+HSHUM = 2.5     # physical_constants.py:26
+REFRH1 = 0.7    # physical_constants.py:27
+
+
+def orographic_vertical_profiles(fsg):
+    """compute_temperature_correction_vertical_profile / ..._humidity_... (orographic_correction.py
+    :18-93): tcorv = fsg^(rgas gamma / (1000 g)) except level 0; qcorv = fsg^(hscale / hshum)
+    except levels 0 and 1."""
+    rgam = RGAS * GAMMA / (1000.0 * GRAV)
+    qexp = HSCALE / HSHUM
+    k = np.arange(fsg.shape[0])
+    tcorv = np.where(k == 0, 0.0, fsg ** rgam).astype(fsg.dtype)
+    qcorv = np.where(k < 2, 0.0, fsg ** qexp).astype(fsg.dtype)
+    return tcorv, qcorv
+
+
+def orographic_horizontal(phis0, fmask, stl, sst):
+    """compute_temperature_correction_horizontal and compute_humidity_correction_horizontal
+    (orographic_correction.py:96-174).  The reference's get_qsat with sig <= 0 divides by the
+    first element of its pressure field (humidity.py:100-101); the caller passes ones there, so
+    that is 1."""
+    dt_ = phis0.dtype.type
+    gamlat = GAMMA / (1000.0 * GRAV)
+    tcorh = gamlat * phis0
+    tsfc = fmask * stl + (1.0 - fmask) * sst
+    tref = tsfc + tcorh
+    pexp = 1000.0 * GRAV / (RGAS * GAMMA)
+    with np.errstate(all="ignore"):
+        psfc = (tsfc / tref) ** pexp
+
+        def esat(ta):
+            return np.where(ta >= 273.16, 6.108e-3 * np.exp(17.269 * (ta - 273.16) / (ta - 35.86)),
+                            6.108e-3 * np.exp(21.875 * (ta - 273.16) / (ta - 7.66)))
+        e_ref = esat(tref)
+        qref = 622.0 * e_ref / (dt_(1.0) - 0.378 * e_ref)
+        qsfc = get_qsat(tsfc, psfc, dt_(1.0))
+    qcorh = REFRH1 * (qref - qsfc)
+    return tcorh.astype(phis0.dtype), qcorh.astype(phis0.dtype)
+
+
+def get_orographic_correction_tendencies(state, data, params, forcing, geometry, rec=None):
+    """get_orographic_correction_tendencies (orographic_correction.py:177-247): the correction
+    tcorh*tcorv (temperature) and qcorh*qcorv (humidity) spread over one model step."""
+    tcorv, qcorv = orographic_vertical_profiles(geometry.fsg)
+    tcorh, qcorh = orographic_horizontal(geometry.phis0, geometry.fmask, forcing.stl_am,
+                                         forcing.sea_surface_temperature)
+    dt = data.date.dt_seconds
+    t = zero_tendency(state.temperature.shape, state.temperature.dtype)
+    t.temperature = (tcorh[None] * tcorv[:, None, None]) / dt
+    t.specific_humidity = (qcorh[None] * qcorv[:, None, None]) / dt
+    return t, data
+
+
+TERMS_OROGRAPHIC = TERMS + [get_orographic_correction_tendencies]
+
+
 def forcing_day_slice(forcing, date):
     """tree_index_3d(forcing, date.model_day()) (speedy_physics.py:119-121, utils.py:104-108)."""
     day = model_day(date)
@@ -1078,17 +1140,18 @@ def forcing_day_slice(forcing, date):
     return f
 
 
-def compute_tendencies(state, forcing, geometry, date, params, rec=None):
+def compute_tendencies(state, forcing, geometry, date, params, rec=None, orographic=False):
     """SpeedyPhysics.compute_tendencies (speedy_physics.py:88-127).
 
-    Tendencies are summed in float ``dtype`` in term order.
+    Tendencies are summed in float ``dtype`` in term order; ``orographic`` appends the
+    orographic correction as the last term.
     """
     kx, ix, il = state.temperature.shape
     dt_ = state.temperature.dtype
     data = zeros_data((ix, il), kx, date, dt_)
     tend = zero_tendency((kx, ix, il), dt_)
     forcing_2d = forcing_day_slice(forcing, date)
-    for term in TERMS:
+    for term in (TERMS_OROGRAPHIC if orographic else TERMS):
         t, data = term(state, data, params, forcing_2d, geometry, rec)
         if t is not None:
             tend.u_wind = tend.u_wind + t.u_wind
@@ -1116,13 +1179,14 @@ def verify_tendencies(state, tend, time_step):
 
 
 def physics_step(state, forcing, geometry, date, params, time_step=None, fuse_verify=True,
-                 rec=None):
+                 rec=None, orographic=False):
     """The physics part of get_physical_tendencies (physics_interface.py:371-376)."""
     if not fuse_verify:
-        return compute_tendencies(state, forcing, geometry, date, params, rec)
+        return compute_tendencies(state, forcing, geometry, date, params, rec, orographic)
     dt_ = state.temperature.dtype.type
     ts = dt_(date.dt_seconds if time_step is None else time_step)
-    tend, data = compute_tendencies(verify_state(state), forcing, geometry, date, params, rec)
+    tend, data = compute_tendencies(verify_state(state), forcing, geometry, date, params, rec,
+                                    orographic)
     return verify_tendencies(state, tend, ts), data
 
 

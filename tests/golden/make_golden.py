@@ -19,7 +19,7 @@ import numpy as np
 
 FILES = ["convection_test.py", "large_scale_condensation_test.py",
          "shortwave_radiation_test.py", "longwave_radiation_test.py", "surface_flux_test.py",
-         "vertical_diffusion_test.py"]
+         "vertical_diffusion_test.py", "orographic_correction_test.py"]
 NPY = ["iptop", "qdif", "cbmf", "precnv", "dfse", "dfqa"]
 
 

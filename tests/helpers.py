@@ -175,8 +175,9 @@ def parity_check(pkg, inst, params=None, max_flip_frac=2e-3, device="cuda", **kw
     args = list(inst.oracle_args(O.default_parameters()))
     rec = O.Margins((inst.ix, inst.il))
     step = O.physics_step if kw.get("fuse_verify") else O.compute_tendencies
-    tend, data = step(*args, rec=rec)
-    ref64 = step(*oracle_f64(inst))
+    oro = bool(kw.get("orographic_correction"))
+    tend, data = step(*args, rec=rec, orographic=oro)
+    ref64 = step(*oracle_f64(inst), orographic=oro)
     rep = compare_fields(got, tend, data, ref64)
     summ = parity_summary(rep, (inst.ix, inst.il), rec.ulps)
     cols = summ.pop("_cols")

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "speedy_derived.h"
 #include "speedy_generic.h"
 #include "speedy_vjp.h"
 
@@ -146,8 +147,11 @@ static int vjp_hand(const spd_vgrid_t& vg, const spd_params_t& p, const HostColu
     ct[1][k] = T(ct_dq[k]);
   }
   spdvjp::Bar<KX, T> b;
+  spd_desc_t d{};  // the orographic profile depends on the level count only
+  d.kx = KX;
+  const spd::Derived D = spd::derive_constants(&d, &vg, &p);
   spdvjp::column_vjp<KX, T>(x, g, T(h.ablco2), T(dt_seconds), T(q_tend_scale), in, ct[0], ct[1],
-                            T(ct_du), T(ct_dv), b);
+                            T(ct_du), T(ct_dv), b, D.qcorv, D.gamlat, D.pexp);
   for (int k = 0; k < KX; ++k) {
     g_t[k] = b.t[k];
     g_q[k] = b.q[k];

@@ -14,6 +14,7 @@ import importlib
 import numpy as np
 import pytest
 
+from tests.test_adjoint_cpu import (VJP_HAND32, VJP_HAND64, vjp_any)
 from tests.test_adjoint_cpu import (HostOut, _flags, _loss_and_grads, build_host, column_of,
                                     run_oracle, structs)
 
@@ -30,10 +31,11 @@ def host(tmp_path_factory):
     return build_host(tmp_path_factory.mktemp("hostcol") / "libhostcol.so")
 
 
-def _gpu_vjp(pkg, inst, cts, fuse_verify=False):
+def _gpu_vjp(pkg, inst, cts, fuse_verify=False, orographic=False):
     import torch
     state, forcing, geom, date = pkg.instance_to_device(inst, "cuda")
-    phys = pkg.SpeedyPhysics(diagnostics=False, fuse_verify=fuse_verify, time_step=1800.0)
+    phys = pkg.SpeedyPhysics(diagnostics=False, fuse_verify=fuse_verify, time_step=1800.0,
+                             orographic_correction=orographic)
     t = lambda a: torch.as_tensor(a, dtype=torch.float32, device="cuda")
     cot = pkg.PhysicsTendency(t(cts["u"]), t(cts["v"]), t(cts["t"]), t(cts["q"]))
     gs, gp = pkg.adjoint.vjp(phys, state, forcing, geom, date, cot)
@@ -43,13 +45,14 @@ def _gpu_vjp(pkg, inst, cts, fuse_verify=False):
                 psa=c(gs.normalized_surface_pressure), u=c(gs.u_wind), v=c(gs.v_wind)), c(gp)
 
 
-CASES = [  # (kx, seed, lfluxland, fused verify with some negative humidity)
-    (8, 708, True, False), (16, 716, True, False), (7, 707, True, False),
-    (8, 808, False, False), (8, 908, True, True), (16, 916, True, True)]
+CASES = [  # (kx, seed, lfluxland, fused verify with some negative humidity, orographic term)
+    (8, 708, True, False, False), (16, 716, True, False, False), (7, 707, True, False, False),
+    (8, 808, False, False, False), (8, 908, True, True, False), (16, 916, True, True, False),
+    (16, 926, True, True, True)]
 
 
-@pytest.mark.parametrize("kx,seed,lfluxland,verify", CASES)
-def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify):
+@pytest.mark.parametrize("kx,seed,lfluxland,verify,oro", CASES)
+def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify, oro):
     inst = pkg.synthetic.land_instance(seed, 32, 16, kx)
     inst.lfluxland = lfluxland
     if verify:
@@ -67,8 +70,8 @@ def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify):
     shape = (kx, inst.ix, inst.il)
     cts = dict(t=rng.normal(size=shape), q=rng.normal(size=shape), u=rng.normal(size=shape),
                v=rng.normal(size=shape))
-    g_gpu, p_gpu = _gpu_vjp(pkg, inst, cts, fuse_verify=verify)
-    flags = _flags(inst) | (16 if verify else 0)
+    g_gpu, p_gpu = _gpu_vjp(pkg, inst, cts, fuse_verify=verify, orographic=oro)
+    flags = _flags(inst) | (16 if verify else 0) | (32 if oro else 0)
     h64 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
     h32 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
     p64 = np.zeros(12)
@@ -79,7 +82,12 @@ def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify):
                   list(cts["q"][:, i, j]) + [0.0] * (16 - kx),
                   float(cts["u"][-1, i, j]), float(cts["v"][-1, i, j]))
             for f32, dst in ((False, h64), (True, h32)):
-                g, _ = _loss_and_grads(host, vg, pr, h, *ct, f32=f32)
+                if oro:  # the taped host forward has no orographic term: the hand-written
+                    # host pass (the kernel's own source) in float64 and float32
+                    g = vjp_any(host, VJP_HAND32 if f32 else VJP_HAND64, vg, pr, h, ct)
+                    g = dict(g, psa=g["psa"][0], u=g["u"][0], v=g["v"][0])
+                else:
+                    g, _ = _loss_and_grads(host, vg, pr, h, *ct, f32=f32)
                 dst["t"][:, i, j], dst["q"][:, i, j], dst["phi"][:, i, j] = g["t"], g["q"], g["phi"]
                 dst["psa"][i, j] = g["psa"]
                 dst["u"][-1, i, j], dst["v"][-1, i, j] = g["u"], g["v"]

@@ -420,3 +420,54 @@ def test_full_chain_finite_on_config0_like_state(params):
     for f in (tend.u_wind, tend.v_wind, tend.temperature, tend.specific_humidity):
         assert np.all(np.isfinite(f))
     assert np.any(tend.temperature != 0)
+
+
+# ---- orographic correction (orographic_correction_test.py) ----------------------------------
+ORO = "orographic_correction_test::test_speedy_fortran_numerical_equivalence::"
+
+
+def test_orographic_profiles_match_fortran(goldens):
+    """test_speedy_fortran_numerical_equivalence (orographic_correction_test.py:279-333): the
+    vertical profiles at 8 levels and the horizontal temperature correction of a 4x4
+    orography against SPEEDY Fortran output, with the reference's tolerances."""
+    _, fsg, *_ = O.vertical_tables(8)
+    tcorv, qcorv = O.orographic_vertical_profiles(fsg)
+    np.testing.assert_allclose(tcorv, g(goldens, ORO + "1"), rtol=1e-3, atol=1e-6)
+    np.testing.assert_allclose(qcorv, g(goldens, ORO + "2"), rtol=1e-3, atol=1e-12)
+    orog = g(goldens, ORO + "0").astype(F32)
+    phis0 = (F32(O.GRAV) * orog).astype(F32)
+    ones = np.ones_like(phis0)
+    tcorh, _ = O.orographic_horizontal(phis0, ones, ones * F32(288.0), ones * F32(285.0))
+    np.testing.assert_allclose(tcorh, g(goldens, ORO + "3"), rtol=1e-3, atol=1e-12)
+    assert tcorv[0] == 0.0 and np.all(tcorv[1:] > 0.0) and np.all(tcorv < 1.0)
+    assert qcorv[0] == 0.0 and qcorv[1] == 0.0 and np.all(qcorv[2:] > 0.0)
+
+
+def test_orographic_tendencies_properties():
+    """test_humidity_horizontal_correction and test_get_orographic_correction_tendencies
+    (orographic_correction_test.py:162-222): on the reference's test setup (Gaussian 1000 m
+    mountain, 70 % land, SST 285 K, land 288 K) the humidity correction is non-zero and bounded,
+    the wind tendencies are zero and the temperature and humidity tendencies are bounded; the
+    tendencies times the step equal the corrections applied to the state (lines 224-257)."""
+    ix, il = 96, 48
+    li, lj = np.meshgrid(np.arange(ix), np.arange(il), indexing="ij")
+    orog = (1000.0 * np.exp(-((li - ix // 2) ** 2 / (2 * (ix / 8) ** 2) +
+                              (lj - il // 2) ** 2 / (2 * (il / 8) ** 2)))).astype(F32)
+    geom = O.make_geometry(ix, il, 8, orog=orog, fmask=np.full((ix, il), 0.7, F32))
+    fo = O.make_forcing((ix, il), sea_surface_temperature=np.full((ix, il), 285.0, F32),
+                        stl_am=np.full((ix, il), 288.0, F32))
+    _, qcorh = O.orographic_horizontal(geom.phis0, geom.fmask, fo.stl_am,
+                                       fo.sea_surface_temperature)
+    assert np.all(np.abs(qcorh) < 10.0) and np.any(qcorh != 0.0)
+    st = O.make_state((8, ix, il))
+    data = O.zeros_data((ix, il), 8, O.make_date())
+    t, _ = O.get_orographic_correction_tendencies(st, data, O.default_parameters(),
+                                                  O.forcing_day_slice(fo, data.date), geom)
+    assert np.all(t.u_wind == 0.0) and np.all(t.v_wind == 0.0)
+    assert np.any(t.temperature != 0.0) and np.any(t.specific_humidity != 0.0)
+    assert np.all(np.abs(t.temperature) < 0.05) and np.all(np.abs(t.specific_humidity) < 0.01)
+    tcorv, qcorv = O.orographic_vertical_profiles(geom.fsg)
+    tcorh, _ = O.orographic_horizontal(geom.phis0, geom.fmask, fo.stl_am,
+                                       fo.sea_surface_temperature)
+    np.testing.assert_allclose(t.temperature * data.date.dt_seconds,
+                               tcorh[None] * tcorv[:, None, None], rtol=1e-4, atol=2e-5)

@@ -51,6 +51,23 @@ def test_seven_levels(pkg):
     check(pkg, inst)
 
 
+@pytest.mark.parametrize("kx", [8, 16])
+def test_orographic_correction(pkg, kx):
+    """The optional last term (orographic_correction.py:177-247) on a land member with
+    orography, against the oracle with the same term."""
+    inst = pkg.synthetic.land_instance(61 + kx, 96, 48, kx)
+    assert inst.phis0.max() > 0
+    check(pkg, inst, orographic_correction=True)
+
+
+def test_orographic_correction_fused_verify(pkg):
+    inst = pkg.synthetic.land_instance(63, 64, 32, 8)
+    rng = np.random.default_rng(3)
+    mask = rng.uniform(size=inst.q.shape) < 0.05
+    inst.q = np.where(mask, -np.abs(inst.q) * 0.01 - 1e-4, inst.q).astype(np.float32)
+    check(pkg, inst, fuse_verify=True, orographic_correction=True, time_step=1800.0)
+
+
 def test_fused_verify_with_negative_humidity(pkg):
     inst = pkg.synthetic.land_instance(9, 64, 32, 8)
     rng = np.random.default_rng(0)
