@@ -51,8 +51,9 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--sections", default="t425,adjoint,serving",
-                    help="extra single-GPU sections: t425, adjoint, serving (comma list, or none)")
+    ap.add_argument("--sections", default="t425,adjoint,serving,held_suarez",
+                    help="extra single-GPU sections: t425, adjoint, serving, held_suarez "
+                         "(comma list, or none)")
     ap.add_argument("--serving-requests", type=int, default=400)
     return ap.parse_args()
 
@@ -350,6 +351,8 @@ def run_b200(args):
             sections["adjoint"] = adjoint_section(pkg, dev)
         if "serving" in wanted:
             sections["serving"] = serving_section(pkg, dev, args.serving_requests)
+        if "held_suarez" in wanted:
+            sections["held_suarez"] = held_suarez_section(pkg, dev, peak, peak_kind)
 
     if rank == 0:
         line = {"metric": "physics columns/s", "value": round(value, 1), "unit": "columns/s",
@@ -389,6 +392,27 @@ def event_ms(fn, reps, warmup=3):
     b.record()
     torch.cuda.synchronize()
     return a.elapsed_time(b) / reps
+
+
+def held_suarez_section(pkg, dev, peak, peak_kind):
+    """Held-Suarez forcing (spd_held_suarez) on T425 with 16 levels: one element-wise launch,
+    HBM-bound; its bytes are u, v, T read and four tendency planes written per level and column
+    plus psa once per column, 4 (7 kx + 1) B per column (370 MB per call, above the L2)."""
+    import torch
+    inst = pkg.synthetic.t425_instance()
+    st, fo, ge, da = pkg.instance_to_device(inst, dev)
+    hs = pkg.HeldSuarezPhysics()
+    out = {k: torch.empty_like(st.temperature) for k in ("u_wind", "v_wind", "temperature",
+                                                          "specific_humidity")}
+    call = lambda: hs.compute_tendencies(st, fo, ge, da, out=out)
+    ms = event_ms(call, 20, warmup=5)
+    cols = inst.columns
+    nbytes = 4 * (7 * inst.kx + 1) * cols
+    bw = nbytes / (ms / 1e3) / 1e9
+    return {"workload": "T425 1280x640, 16 levels, one instance", "columns": cols,
+            "ms_per_call": round(ms, 4), "columns_per_s": round(cols / (ms / 1e3), 1),
+            "algorithmic_bytes_per_call": nbytes, "hbm_gbs": round(bw, 1), "peak_gbs": peak,
+            "peak_kind": peak_kind, "hbm_frac": round(bw / peak, 4), "kernel": "hs_vec4"}
 
 
 def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):

@@ -157,6 +157,33 @@ int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_p
 int spd_preload(void);
 
 /* ----------------------------------------------------------------------------------------- */
+/* Held-Suarez forcing: HeldSuarezPhysics.compute_tendencies                                 */
+/*   (jcm/physics/held_suarez/held_suarez_physics.py:76-101), the reference's second physics */
+/* package, per element: Newtonian relaxation of T towards the radiative-equilibrium          */
+/* temperature (equilibrium_temperature, :53-62; kt, :70-74) and Rayleigh drag on u and v     */
+/* below sigma_b (kv, :64-68); the humidity tendency is zero.  Units are the caller's: rates   */
+/* in 1/s and temperatures in K give tendencies in K/s and m/s^2 (the reference passes them    */
+/* nondimensionalized by dinosaur's scales; the arithmetic is the same).                     */
+/* ----------------------------------------------------------------------------------------- */
+typedef struct {
+  int32_t kx, ix, il, reserved;
+  float sigma_b;          /* boundary-layer top (sigma) */
+  float kf, ka, ks;       /* friction, free-atmosphere and surface relaxation rates */
+  float min_t, max_t;     /* bounds of the equilibrium temperature */
+  float dt_y, dthz;       /* its horizontal and vertical variations */
+  float kappa;            /* R / cp */
+  float sigma[SPD_MAX_KX];  /* level centres, top to bottom (coords.vertical.centers) */
+} spd_hs_desc_t;
+
+/* Latitude tables for spd_held_suarez: lat_tab[0][j] = sin(lat_j)^2, lat_tab[1][j] =
+ * cos(lat_j)^2, lat_tab[2][j] = cos(lat_j)^4 (as the reference forms them), j < il, on the
+ * device.  u, v, t are [kx][C] (C = ix*il), psa [C]; du, dv, dt, dq [kx][C], overlapping
+ * neither the inputs nor one another (SPD_ERR_ALIAS). */
+int spd_held_suarez(const spd_hs_desc_t* desc, const float* lat_tab, const float* u,
+                    const float* v, const float* t, const float* psa, float* du, float* dv,
+                    float* dt, float* dq, void* stream);
+
+/* ----------------------------------------------------------------------------------------- */
 /* Adjoint (vector-Jacobian product) of the plain forward.                                    */
 /* Replaces jax.vjp of SpeedyPhysics.compute_tendencies (speedy_physics.py:88-127; the         */
 /* reference differentiates through jax.checkpoint-ed terms, speedy_physics.py:82-86).         */

@@ -120,6 +120,13 @@ class SpeedyLibraryError(RuntimeError):
     pass
 
 
+class HsDesc(C.Structure):
+    _fields_ = [("kx", C.c_int32), ("ix", C.c_int32), ("il", C.c_int32), ("reserved", C.c_int32),
+                ("sigma_b", C.c_float), ("kf", C.c_float), ("ka", C.c_float), ("ks", C.c_float),
+                ("min_t", C.c_float), ("max_t", C.c_float), ("dt_y", C.c_float),
+                ("dthz", C.c_float), ("kappa", C.c_float), ("sigma", C.c_float * 16)]
+
+
 def _declare(lib):
     P = C.POINTER
     lib.spd_fwd_scratch_bytes.argtypes = [P(Desc)]
@@ -163,6 +170,8 @@ def _declare(lib):
     lib.spd_ensemble_vjp.argtypes = [P(Class), C.c_int, C.c_void_p, P(PlanInfo), C.c_int,
                                      C.c_void_p]
     lib.spd_ensemble_vjp.restype = C.c_int
+    lib.spd_held_suarez.argtypes = [P(HsDesc)] + [C.c_void_p] * 10
+    lib.spd_held_suarez.restype = C.c_int
     for name, spec in EXTRA_DECLS.items():
         fn = getattr(lib, name, None)
         if fn is not None:

@@ -13,7 +13,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu", "csrc/speedy_ensemble.cu",
-           "csrc/speedy_adjoint.cu"]
+           "csrc/speedy_adjoint.cu", "csrc/held_suarez.cu"]
 HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
            "csrc/speedy_kernels.cuh", "csrc/speedy_ensemble.cuh", "csrc/speedy_ad.h",
            "csrc/speedy_generic.h", "csrc/speedy_vjp.h",

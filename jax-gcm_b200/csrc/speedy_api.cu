@@ -132,6 +132,7 @@ int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_ou
 
 int preload_ensemble();
 int preload_adjoint();
+int preload_held_suarez();
 
 }  // namespace spd
 
@@ -140,7 +141,8 @@ extern "C" {
 int spd_preload(void) {
   const int b = spd::preload_ensemble();
   const int c = spd::preload_adjoint();
-  return (b == SPD_OK && c == SPD_OK) ? SPD_OK : SPD_ERR_CUDA;
+  const int h = spd::preload_held_suarez();
+  return (b == SPD_OK && c == SPD_OK && h == SPD_OK) ? SPD_OK : SPD_ERR_CUDA;
 }
 
 
