@@ -54,11 +54,17 @@ enum spd_flags {
   SPD_LSKINEB = 1u << 2,      /* SurfaceFluxParameters.lskineb (params.py:181) */
   SPD_INCREASE_CO2 = 1u << 3, /* ForcingParameters.increase_co2 (params.py:34) */
   SPD_FUSE_VERIFY = 1u << 4,  /* apply verify_state before and verify_tendencies after */
-  SPD_OROGRAPHIC = 1u << 5    /* orographic correction as the last term (orographic_correction.py
+  SPD_OROGRAPHIC = 1u << 5,   /* orographic correction as the last term (orographic_correction.py
                                  :177-247; commented out of the reference's term list at
                                  speedy_physics.py:65,79).  Its tendency divides by
                                  spd_desc_t.dt_seconds, which must then equal
                                  DateData.dt_seconds. */
+  SPD_ACCUMULATE_DIAGNOSTICS = 1u << 6
+  /* The forward adds precnv, precls and every non-NULL float diagnostic to what the output
+   * buffers hold (out[c] += value) instead of overwriting them; the tendency planes and the
+   * integer levels are written as usual.  This is DiagnosticsCollector's running average
+   * (jcm/model.py:46-64: data[i] += new / steps) without a pass over PhysicsData per physics
+   * step: zero the buffers, make the steps' calls, scale by 1/steps once. */
 };
 
 /* One grid instance: shape, switches and DateData (jcm/date.py:9-14). */

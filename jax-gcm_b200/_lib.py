@@ -20,6 +20,7 @@ SPD_LSKINEB = 1 << 2
 SPD_INCREASE_CO2 = 1 << 3
 SPD_FUSE_VERIFY = 1 << 4
 SPD_OROGRAPHIC = 1 << 5
+SPD_ACCUMULATE_DIAGNOSTICS = 1 << 6
 
 
 class Desc(C.Structure):

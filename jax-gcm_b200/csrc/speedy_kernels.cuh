@@ -117,8 +117,13 @@ __device__ __forceinline__ uint32_t first_process(const ConstsD& CD, const spd_i
   out.v_wind[(size_t)ST_CLSTR * C + c] = o.clstr;
   out.v_wind[(size_t)ST_IPTOP * C + c] = __int_as_float(o.iptop);
   out.v_wind[(size_t)ST_ICLTOP * C + c] = __int_as_float(o.icltop);
-  __stcs(out.precnv + c, o.precnv);
-  __stcs(out.precls + c, o.precls);
+  if (CD.K.flags & SPD_ACCUMULATE_DIAGNOSTICS) {
+    out.precnv[c] = out.precnv[c] + o.precnv;
+    out.precls[c] = out.precls[c] + o.precls;
+  } else {
+    __stcs(out.precnv + c, o.precnv);
+    __stcs(out.precls + c, o.precls);
+  }
   return 1u << min(max(o.icltop, 0), KX - 1);
 }
 
@@ -213,19 +218,24 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
     const float dq = dqp[k * kNT];
     __stcs(out.specific_humidity + i, qs != 1.0f ? dq * qs : dq);
   }
-  if (out.cbmf) out.cbmf[c] = o.cbmf;
-  if (out.cloudc) out.cloudc[c] = o.cloudc;
-  if (out.cloudstr) out.cloudstr[c] = o.clstr;
-  if (out.rsds) out.rsds[c] = o.rsds;
-  if (out.rsns) out.rsns[c] = o.rsns;
-  if (out.ftop_sw) out.ftop_sw[c] = o.ftop_sw;
-  if (out.rlds) out.rlds[c] = o.rlds;
-  if (out.rlns) out.rlns[c] = o.rlns;
-  if (out.ftop_lw) out.ftop_lw[c] = o.ftop_lw;
-  if (out.tsfc) out.tsfc[c] = o.tsfc;
-  if (out.tskin) out.tskin[c] = o.tskin;
-  if (out.shf) out.shf[c] = o.shf;
-  if (out.evap) out.evap[c] = o.evap;
+  // diagnostics: stored, or added to the caller's sums under SPD_ACCUMULATE_DIAGNOSTICS
+  const bool acc = (K.flags & SPD_ACCUMULATE_DIAGNOSTICS) != 0;
+  auto put = [&](float* f, float x) {
+    if (f) f[c] = acc ? f[c] + x : x;
+  };
+  put(out.cbmf, o.cbmf);
+  put(out.cloudc, o.cloudc);
+  put(out.cloudstr, o.clstr);
+  put(out.rsds, o.rsds);
+  put(out.rsns, o.rsns);
+  put(out.ftop_sw, o.ftop_sw);
+  put(out.rlds, o.rlds);
+  put(out.rlns, o.rlns);
+  put(out.ftop_lw, o.ftop_lw);
+  put(out.tsfc, o.tsfc);
+  put(out.tskin, o.tskin);
+  put(out.shf, o.shf);
+  put(out.evap, o.evap);
   if (out.iptop) out.iptop[c] = o.iptop;
   if (out.icltop) out.icltop[c] = o.icltop;
 }

@@ -473,11 +473,16 @@ class SpeedyPhysics(Physics):
         return buf
 
     def compute_tendencies(self, state: PhysicsState, forcing: ForcingData, geometry: Geometry,
-                           date: DateData, out: Optional[dict] = None, marker=None):
+                           date: DateData, out: Optional[dict] = None, marker=None,
+                           accumulate: bool = False):
         """Tendencies and PhysicsData for ``state``.  ``out`` may give preallocated output
         tensors (they must not overlap the inputs); ``marker`` (a torch.cuda.Event) is recorded
         between the two launches (the first and second halves of the column physics), for
-        timing them separately."""
+        timing them separately.  ``accumulate=True`` adds precnv, precls and the float
+        diagnostics to what ``out`` holds instead of overwriting them (the running sums of
+        DiagnosticsCollector, jcm/model.py:46-64; scale by 1/steps once at the end)."""
+        if accumulate and out is None:
+            raise ValueError("accumulate=True adds into `out`: pass the running sums")
         lib = _lib.load()
         kx, ix, il = geometry.nodal_shape
         t = state.temperature
@@ -514,6 +519,8 @@ class SpeedyPhysics(Physics):
         outs = _lib.Outputs(**{k: (out[k].data_ptr() if k in out else None)
                                for k in _lib.OUTPUT_FIELDS})
         desc = self.desc(geometry, date, forcing.lfluxland)
+        if accumulate:
+            desc.flags |= _lib.SPD_ACCUMULATE_DIAGNOSTICS
         scratch = self._scratch_for(desc, dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
         ev = C.c_void_p(marker.cuda_event) if marker is not None else None

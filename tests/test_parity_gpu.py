@@ -95,3 +95,40 @@ def test_diagnostics_and_levels(pkg):
     inst = pkg.synthetic.land_instance(21, 96, 48, 8)
     rep, _ = check(pkg, inst)
     assert rep["icltop"]["nbad"] == 0 and rep["iptop"]["nbad"] == 0
+
+
+def test_accumulated_diagnostics_equal_the_sum_of_calls(pkg):
+    """SPD_ACCUMULATE_DIAGNOSTICS: two accumulating calls (shortwave on, then off) into zeroed
+    buffers give exactly the sum of the two plain calls' diagnostics; the tendencies are the
+    second call's own."""
+    import dataclasses
+    import torch
+    inst = pkg.synthetic.land_instance(71, 64, 32, 16)
+    st, fo, ge, da = pkg.instance_to_device(inst, "cuda")
+    phys = pkg.SpeedyPhysics()
+    dates = [da, dataclasses.replace(da, model_step=int(da.model_step) + 1)]
+    plain = []
+    for d in dates:
+        tend, data = phys.compute_tendencies(st, fo, ge, d)
+        plain.append((tend, data))
+    kx, ix, il = inst.kx, inst.ix, inst.il
+    e3 = lambda: torch.empty((kx, ix, il), dtype=torch.float32, device="cuda")
+    out = dict(u_wind=e3(), v_wind=e3(), temperature=e3(), specific_humidity=e3())
+    diag = ("precnv", "precls") + pkg.physics.DIAG_2D
+    for n in diag:
+        out[n] = torch.zeros((ix, il), dtype=torch.float32, device="cuda")
+    for n in ("iptop", "icltop"):
+        out[n] = torch.empty((ix, il), dtype=torch.int32, device="cuda")
+    for d in dates:
+        tend, _ = phys.compute_tendencies(st, fo, ge, d, out=out, accumulate=True)
+    torch.cuda.synchronize()
+    assert torch.equal(tend.temperature, plain[1][0].temperature)
+    flat = lambda data: {"precnv": data.convection.precnv, "precls": data.condensation.precls,
+                         "rsds": data.shortwave_rad.rsds, "cloudc": data.shortwave_rad.cloudc,
+                         "rlds": data.surface_flux.rlds, "evap": data.surface_flux.evap,
+                         "ftop_lw": data.longwave_rad.ftop}
+    a, b = flat(plain[0][1]), flat(plain[1][1])
+    for k in a:
+        assert torch.equal(out[k], a[k] + b[k]), k
+    with pytest.raises(ValueError):
+        phys.compute_tendencies(st, fo, ge, da, accumulate=True)
