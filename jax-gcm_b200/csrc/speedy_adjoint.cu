@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kBlock)
   prepass_tiles(A, members, tiles, ntiles);
 }
 
-__global__ void __launch_bounds__(kAdjBlock, 3)
+__global__ void __launch_bounds__(kAdjBlock, 4)
     ensemble_adjoint(const __grid_constant__ VjpClassArgs A,
                      const VjpMemberDev* __restrict__ members, const Tile* __restrict__ tiles,
                      int ntiles) {
