@@ -123,14 +123,15 @@ class Ensemble:
         return [m.out for m in self.members]
 
     def autotune(self, candidates=None, reps=5):
-        """Picks the persistent grid size by timing the candidates (CUDA events); cached per
-        ensemble signature."""
+        """Picks the launch shape by timing the candidates (CUDA events): persistent grids of
+        0 (SMs x resident blocks), 1-4 blocks per SM, or one block per tile
+        (``_lib.GRID_PER_TILE``); cached per ensemble signature."""
         sig = self.signature()
         if sig in _TUNE_CACHE:
             self.grid_blocks = _TUNE_CACHE[sig]
             return self.grid_blocks
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        cands = candidates or [0, sms, 2 * sms, 3 * sms, 4 * sms]
+        cands = candidates or [0, sms, 2 * sms, 3 * sms, 4 * sms, _lib.GRID_PER_TILE]
         best, best_ms = 0, float("inf")
         for gb in cands:
             self.forward(gb)

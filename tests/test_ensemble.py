@@ -126,7 +126,7 @@ def test_ensemble_graph_replay_and_autotune(pkg):
         for k in r:
             assert torch.equal(o[k], r[k]), k
     gb = ens.autotune(reps=2)
-    assert gb >= 0
+    assert gb >= 0 or gb == pkg._lib.GRID_PER_TILE
     for o in ens.forward():
         for v in o.values():
             v.fill_(float("nan"))
