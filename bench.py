@@ -217,8 +217,8 @@ def run_b200(args):
             ms = float(t.item())
         return ms
 
-    # The timed region: K steps between two events, with a marker event between the two
-    # launches of every step (batched mode) so that the second launch is timed alone.
+    # The timed region: K steps between two events.  A second pass records a marker event
+    # between the two launches of every step (batched mode) so that each launch is timed alone.
     marks = [(primed_event(), primed_event(), primed_event()) for _ in range(args.steps)]
     for _ in range(args.warmup):
         step()
@@ -230,17 +230,20 @@ def run_b200(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    for (a, m, b) in marks:
-        if ens is not None:
-            a.record()
-            step(marker=m)
-            b.record()
-        else:
-            step()
+    for _ in range(args.steps):
+        step()
     e1.record()
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
+    # the two launches timed apart, in a separate pass of as many steps (a marker event between
+    # them serialises them in plain stream order; the timed steps above overlap them)
+    if ens is not None:
+        for (a, m, b) in marks:
+            a.record()
+            step(marker=m)
+            b.record()
+        torch.cuda.synchronize()
     total_ms = e0.elapsed_time(e1)
     if dist is not None:
         t = torch.tensor([total_ms], device=dev)
@@ -437,7 +440,8 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
         call(marker=m)
         b.record()
     torch.cuda.synchronize()
-    call_ms = sum(a.elapsed_time(b) for (a, m, b) in marks) / reps
+    marked_ms = sum(a.elapsed_time(b) for (a, m, b) in marks) / reps
+    call_ms = event_ms(call, reps)  # the drop-in call as used: the two launches overlapped
     first_ms = sum(a.elapsed_time(m) for (a, m, b) in marks) / reps
     col_ms = sum(m.elapsed_time(b) for (a, m, b) in marks) / reps
     # 24 calls in one graph
@@ -458,7 +462,9 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
     bw = b2 / (col_ms / 1e3) / 1e9
     out_d = {"workload": "T425 1280x640, 16 levels, one instance", "columns": cols,
              "path_algorithmic_bytes_per_call": nbytes,
-             "plain_call_ms": round(call_ms, 4), "first_launch_ms": round(first_ms, 4),
+             "plain_call_ms": round(call_ms, 4),
+             "plain_call_launches_apart_ms": round(marked_ms, 4),
+             "first_launch_ms": round(first_ms, 4),
              "second_launch_ms": round(col_ms, 4),
              "graph_24_calls_ms_per_call": round(graph_ms, 4),
              "columns_per_s_plain": round(cols / (call_ms / 1e3), 1),

@@ -151,7 +151,9 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 
 /* Timing hook (no reference counterpart): spd_fwd, recording `event` (a cudaEvent_t, or NULL)
  * on `stream` between its two launches, so that a caller can time them separately with
- * events. */
+ * events.  With an event the launches run in plain stream order; without one (and in spd_fwd)
+ * the second launch is a programmatic dependent launch that starts as the first one's blocks
+ * retire and waits on the device for its completion before reading its results. */
 int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
                    const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
                    size_t scratch_bytes, void* stream, void* event);
@@ -279,7 +281,8 @@ int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 
 /* Timing hook (no reference counterpart): spd_ensemble_fwd, recording `event` (a cudaEvent_t,
- * or NULL) on `stream` between its two launches (the first and the second half). */
+ * or NULL) on `stream` between its two launches (the first and the second half), which then
+ * run in plain stream order (see spd_fwd_marked). */
 int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
                             const spd_plan_info_t* info, int grid_blocks, void* stream,
                             void* event);

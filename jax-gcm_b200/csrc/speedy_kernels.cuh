@@ -150,11 +150,17 @@ __device__ __forceinline__ void orographic_horizontal(const Derived& D, float ph
 template <int KX>
 __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
                                                const spd_inputs_t& in, const spd_outputs_t& out,
-                                               uint32_t Sw, const ZonalRow* __restrict__ table,
-                                               int c, int C, int il) {
+                                               const uint32_t* S,
+                                               const ZonalRow* __restrict__ table, int c, int C,
+                                               int il) {
   const Consts& K = CD.K;
   const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
   const uint32_t neg = load_state<KX>(sm, in, verify, c, C);
+  // Everything below reads the first launch's results (stage, level set, solar table).  When
+  // this launch overlaps the first one's tail (programmatic dependent launch), wait here for
+  // its completion; otherwise the first launch is complete already and this returns at once.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const uint32_t Sw = *S;
   float* qsp = sm + (size_t)A_QSAT * KX * kNT + threadIdx.x;
   float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
   float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
