@@ -40,6 +40,16 @@ def test_land_member(pkg, kx):
     check(pkg, inst)
 
 
+def test_large_member_flip_statistics(pkg):
+    """T85 with 16 levels (32,768 columns, land, orography, sea ice): the more columns, the
+    likelier a convection or condensation trigger within a few float32 ulps of its threshold;
+    every column outside the bar must be such a flip (explained by the oracle's recorded
+    margins), and at most 0.2 % of the columns may flip (measured: none)."""
+    inst = pkg.synthetic.land_instance(85, 256, 128, 16, sst_noise=1.5)
+    _, summ = check(pkg, inst)
+    assert summ["columns"] == 256 * 128
+
+
 def test_land_member_with_sea_ice(pkg):
     inst = pkg.synthetic.land_instance(5, 128, 64, 8, sst_noise=1.5)
     assert inst.sice.sum() > 0
