@@ -140,6 +140,16 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time (every rank takes this collective at the same point)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_b200(args):
     import torch
     pkg = importlib.import_module("jax-gcm_b200")
@@ -210,12 +220,7 @@ def run_b200(args):
         e1.record()
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
     # The timed region: K steps between two events.  A second pass records a marker event
     # between the two launches of every step (batched mode) so that each launch is timed alone.
@@ -244,11 +249,7 @@ def run_b200(args):
             step(marker=m)
             b.record()
         torch.cuda.synchronize()
-    total_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = total_ms / args.steps
     col_ms = pre_ms = None
     if ens is not None:
