@@ -161,3 +161,133 @@ class Ensemble:
             for _ in range(calls):
                 self.forward()
         return g
+
+
+STATE_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential",
+                "normalized_surface_pressure")
+RESULT_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity", "precnv", "precls")
+
+
+def _packed_layout(members, fields, level_fields):
+    """Offsets (in floats, each field 64-float aligned) of every member's fields in one flat
+    buffer; returns ([{field: (offset, shape)}], total floats)."""
+    off, out = 0, []
+    for m in members:
+        kx, ix, il = m.geometry.nodal_shape
+        d = {}
+        for f in fields:
+            shape = (kx, ix, il) if f in level_fields else (ix, il)
+            n = 1
+            for s in shape:
+                n *= s
+            d[f] = (off, shape)
+            off += (n + 63) // 64 * 64
+        out.append(d)
+    return out, off
+
+
+class HostPipeline:
+    """Ensemble steps whose state comes from, and whose results go to, pinned host memory.
+
+    Every member's state (u, v, T, q, phi, psa) lives in one packed host buffer and every
+    member's results (the four tendency planes, precnv, precls) in another, so a step is one
+    host-to-device copy, one ``spd_ensemble_fwd`` and one device-to-host copy.  ``depth`` sets of
+    device buffers (each with its own plan) rotate over three streams: while step n computes,
+    step n+1's state uploads and step n-1's results download (PCIe carries both directions at
+    once).  Forcing and geometry stay resident.
+
+    ``host_state`` (pack into it with ``set_state``) is read by every step; ``submit()`` enqueues
+    one step and returns the index of the host result buffer it writes; ``wait(i)`` blocks until
+    that buffer is complete and ``results(i)`` views it per member.
+    """
+
+    def __init__(self, members: List[Member], date, depth: int = 2, **ensemble_kw):
+        dev = members[0].state.temperature.device
+        self.device, self.depth = dev, depth
+        level = {"u_wind", "v_wind", "temperature", "specific_humidity", "geopotential"}
+        self.in_layout, n_in = _packed_layout(members, STATE_FIELDS, level)
+        self.out_layout, n_out = _packed_layout(members, RESULT_FIELDS, level)
+        self.host_state = torch.empty(n_in, dtype=torch.float32, pin_memory=True)
+        self.host_results = [torch.empty(n_out, dtype=torch.float32, pin_memory=True)
+                             for _ in range(depth)]
+        self.dev_state = [torch.empty(n_in, dtype=torch.float32, device=dev)
+                          for _ in range(depth)]
+        self.dev_results = [torch.empty(n_out, dtype=torch.float32, device=dev)
+                            for _ in range(depth)]
+        self.ensembles = []
+        for b in range(depth):
+            mem = []
+            for m, li, lo in zip(members, self.in_layout, self.out_layout):
+                sv = {f: self._view(self.dev_state[b], *li[f]) for f in STATE_FIELDS}
+                ov = {f: self._view(self.dev_results[b], *lo[f]) for f in RESULT_FIELDS}
+                st = type(m.state)(*(sv[f] for f in STATE_FIELDS))
+                mem.append(Member(st, m.forcing, m.geometry, ov))
+            self.ensembles.append(Ensemble(mem, date, **ensemble_kw))
+        self.h2d = torch.cuda.Stream(dev)
+        self.compute = torch.cuda.Stream(dev)
+        self.d2h = torch.cuda.Stream(dev)
+        ev = lambda: [torch.cuda.Event() for _ in range(depth)]
+        self.uploaded, self.computed, self.downloaded = ev(), ev(), ev()
+        self.used = [False] * depth
+        self.n = 0
+
+    @staticmethod
+    def _view(flat, off, shape):
+        n = 1
+        for s in shape:
+            n *= s
+        return flat[off:off + n].view(shape)
+
+    def set_state(self, i, state):
+        """Packs member i's state (a PhysicsState of CPU or CUDA tensors) into host_state."""
+        for f in STATE_FIELDS:
+            self._view(self.host_state, *self.in_layout[i][f]).copy_(getattr(state, f))
+
+    def begin(self):
+        """Orders the pipeline's streams after the work already on the current stream."""
+        cur = torch.cuda.current_stream(self.device)
+        for s in (self.h2d, self.compute, self.d2h):
+            s.wait_stream(cur)
+
+    def submit(self):
+        b = self.n % self.depth
+        if self.used[b]:
+            self.h2d.wait_event(self.computed[b])      # the buffer's previous step read it
+        with torch.cuda.stream(self.h2d):
+            self.dev_state[b].copy_(self.host_state, non_blocking=True)
+            self.uploaded[b].record(self.h2d)
+        self.compute.wait_event(self.uploaded[b])
+        if self.used[b]:
+            self.compute.wait_event(self.downloaded[b])  # its previous results were read out
+        with torch.cuda.stream(self.compute):
+            self.ensembles[b].forward()
+            self.computed[b].record(self.compute)
+        self.d2h.wait_event(self.computed[b])
+        with torch.cuda.stream(self.d2h):
+            self.host_results[b].copy_(self.dev_results[b], non_blocking=True)
+            self.downloaded[b].record(self.d2h)
+        self.used[b] = True
+        self.n += 1
+        return b
+
+    def end(self):
+        """Orders the current stream after every submitted step."""
+        cur = torch.cuda.current_stream(self.device)
+        for s in (self.h2d, self.compute, self.d2h):
+            cur.wait_stream(s)
+
+    def wait(self, i):
+        self.downloaded[i].synchronize()
+
+    def results(self, i):
+        """Member views of host result buffer i: [{field: tensor}] (valid after wait(i))."""
+        return [{f: self._view(self.host_results[i], *lo[f]) for f in RESULT_FIELDS}
+                for lo in self.out_layout]
+
+    @property
+    def h2d_bytes(self):
+        return self.host_state.numel() * 4
+
+    @property
+    def d2h_bytes(self):
+        return self.host_results[0].numel() * 4

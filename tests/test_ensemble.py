@@ -136,3 +136,29 @@ def test_ensemble_graph_replay_and_autotune(pkg):
     for o, r in zip([m.out for m in ens.members], ref):
         for k in r:
             assert torch.equal(o[k], r[k]), k
+
+
+@pytest.mark.gpu
+def test_host_pipeline_matches_ensemble(pkg):
+    """HostPipeline (state from and results to pinned host memory, steps overlapped over
+    double buffers) gives every member the results Ensemble.forward gives, bitwise, on each of
+    three consecutive steps (both buffer sets, one reused)."""
+    import torch
+    insts, members, plain = _members(pkg, "cuda")
+    ref = [{k: v.clone() for k, v in o.items()}
+           for o in pkg.Ensemble(members, plain[0][3]).forward()]
+    pipe = pkg.batched.HostPipeline(
+        [pkg.Member(m.state, m.forcing, m.geometry) for m in members], plain[0][3])
+    for i, m in enumerate(members):
+        pipe.set_state(i, m.state)
+    pipe.begin()
+    bufs = [pipe.submit() for _ in range(3)]
+    pipe.end()
+    torch.cuda.synchronize()
+    assert bufs == [0, 1, 0]
+    for b in (0, 1):
+        pipe.wait(b)
+        for got, want in zip(pipe.results(b), ref):
+            for k in want:
+                assert torch.equal(got[k], want[k].cpu()), k
+    assert pipe.h2d_bytes > 0 and pipe.d2h_bytes > 0
