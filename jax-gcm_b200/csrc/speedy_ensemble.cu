@@ -17,6 +17,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "speedy_ensemble.cuh"
@@ -103,17 +104,20 @@ struct Residency {
   int sms = 0, moist = 0, cols[17] = {};  // resident blocks per SM; cols by arena level count
 };
 
-// SMs and resident blocks per SM of both kernels (once per process; idempotent, so races are
-// harmless).
+// SMs and resident blocks per SM of both kernels on the current device, set up once per device
+// (the shared-memory attribute of a kernel is a per-device setting).
 int residency(Residency& R) {
-  static Residency cached;
-  static bool done = false;
-  if (!done) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static Residency cached[kMaxDevices];
+  static bool done[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPD_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done[dev]) {
     Residency r;
-    int dev = 0;
     if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes<16>()) != cudaSuccess ||
-        cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.moist, ensemble_moist, kNT, 0) !=
             cudaSuccess)
@@ -124,10 +128,10 @@ int residency(Residency& R) {
         return SPD_ERR_CUDA;
     r.moist = std::max(r.moist, 1);
     for (int kx : {7, 8, 16}) r.cols[kx] = std::max(r.cols[kx], 1);
-    cached = r;
-    done = true;
+    cached[dev] = r;
+    done[dev] = true;
   }
-  R = cached;
+  R = cached[dev];
   return SPD_OK;
 }
 }  // namespace
