@@ -275,6 +275,27 @@ def test_run_loop_real_time_with_fake_device():
     assert all(r.t_done >= r.arrival for r in fin)
 
 
+def test_run_freezes_the_collector_for_its_duration():
+    import gc
+    src, _ = make_source(a=(8, 64, 32))
+    seen = []
+
+    class Probe(FakeBackend):
+        def launch(self, kind, reqs, devs):
+            seen.append(gc.get_freeze_count())
+            return super().launch(kind, reqs, devs)
+
+    reqs = lambda: [S.Request(S.TENDENCY, ["a"], arrival=0.001 * i) for i in range(4)]
+    n_objects = len(gc.get_objects())
+    S.Scheduler(Probe(per_col=1e-8, realtime=True), src, 1 << 30).run(reqs(), timeout_s=30)
+    assert seen and min(seen) >= n_objects // 2   # objects alive at the start were frozen
+    assert gc.get_freeze_count() == 0             # and released at the end
+    seen.clear()
+    S.Scheduler(Probe(per_col=1e-8, realtime=True), src, 1 << 30,
+                freeze_gc=False).run(reqs(), timeout_s=30)
+    assert seen and max(seen) == 0
+
+
 def test_poisson_stream_shape():
     reqs = S.poisson_stream(seed=4, rate=200.0, n=2000)
     t = np.array([r.arrival for r in reqs])
