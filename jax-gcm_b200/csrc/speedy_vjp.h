@@ -24,6 +24,16 @@
 #include "speedy_b200.h"
 #include "speedy_generic.h"
 
+// The per-level loops stay rolled (SPD_ROLL); the loops over the four longwave bands (and the
+// parameter adjoints) are unrolled on the device, so that their small arrays (band fluxes,
+// transmissivities, blackbody fractions and their adjoints) are registers rather than local
+// memory.
+#if defined(__CUDA_ARCH__)
+#define SPD_BANDS _Pragma("unroll")
+#else
+#define SPD_BANDS
+#endif
+
 namespace spdvjp {
 
 using spdgen::ColumnIn;
@@ -928,7 +938,7 @@ SPD_HD void lw_level(const Ctx& x, const Col<KX, F>& c, int k, F ablco2, LwLevel
   F a[4];
   lw_absorb(x, c, k, ablco2, a);
   const F dh = F(x.vg->dhs[k]);
-  SPD_ROLL
+  SPD_BANDS
   for (int b = 0; b < 4; ++b) L.tau[b] = fexp(-a[b] * c.psa * dh);
   const F sbc = F(5.67e-8);
   if (k == 0) {
@@ -955,7 +965,7 @@ SPD_HD void longwave_down(const Ctx& x, Col<KX, F>& c, F ablco2, Lw<KX, F>& w) {
   LwLevel<F> L;
   lw_level(x, c, 0, ablco2, L);
   radset_d(c.t[0], F(p.epslw), fb, dfb);
-  SPD_ROLL
+  SPD_BANDS
   for (int b = 0; b < 4; ++b) {
     const F emis = F(1) - L.tau[b];
     w.fld[0][b] = emis * (fb[b] * (L.st0 + emis * L.st1));
@@ -968,7 +978,7 @@ SPD_HD void longwave_down(const Ctx& x, Col<KX, F>& c, F ablco2, Lw<KX, F>& w) {
   for (int k = 1; k < KX; ++k) {
     lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
-    SPD_ROLL
+    SPD_BANDS
     for (int b = 0; b < 4; ++b) {
       const F emis = F(1) - L.tau[b];
       w.fld[k][b] = L.tau[b] * w.fld[k - 1][b] + emis * (fb[b] * (L.st0 + emis * L.st1));
@@ -996,7 +1006,7 @@ SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, F ablc
   LwLevel<F> L;
   radset_d(c.tsfc, F(p.epslw), fb, dfb);
   const F fsw[4] = {c.fsw0, c.fsw1, F(0), F(0)};
-  SPD_ROLL
+  SPD_BANDS
   for (int b = 0; b < 4; ++b) w.flu[KX][b] = fb[b] * c.rlus2 + refsfc * fsw[b];
   c.dfl[KX - 1] = c.dfl[KX - 1] + F(p.epslw) * c.rlus2;
   F sk = ((w.flu[KX][0] + w.flu[KX][1]) + w.flu[KX][2]) + w.flu[KX][3];
@@ -1004,7 +1014,7 @@ SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, F ablc
   for (int k = KX - 1; k >= 1; --k) {
     lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
-    SPD_ROLL
+    SPD_BANDS
     for (int b = 0; b < 4; ++b) {
       const F emis = F(1) - L.tau[b];
       w.flu[k][b] = L.tau[b] * w.flu[k + 1][b] + emis * (fb[b] * (L.st0 - emis * L.st1));
@@ -1016,7 +1026,7 @@ SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, F ablc
   lw_level(x, c, 0, ablco2, L);
   radset_d(c.t[0], F(p.epslw), fb, dfb);
   F top[2];
-  SPD_ROLL
+  SPD_BANDS
   for (int b = 0; b < 2; ++b) {
     const F emis = F(1) - L.tau[b];
     top[b] = L.tau[b] * w.flu[1][b] + emis * (fb[b] * (L.st0 - emis * L.st1));
@@ -1062,7 +1072,7 @@ SPD_HD void lw_level_rev(const Ctx& x, const Col<KX, F>& c, int k, F ablco2,
   lw_absorb(x, c, k, ablco2, a);
   const F dh = F(x.vg->dhs[k]);
   F ab[4];
-  SPD_ROLL
+  SPD_BANDS
   for (int bb = 0; bb < 4; ++bb) {
     const F Eb = tau_b[bb] * L.tau[bb];
     ab[bb] = -Eb * c.psa * dh;
@@ -1151,7 +1161,7 @@ SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow&
     radset_d(c.t[0], F(p.epslw), fb, dfb);
     F tb[4] = {F(0), F(0), F(0), F(0)};
     F s0b = st0b_0, s1b = F(0);
-    SPD_ROLL
+    SPD_BANDS
     for (int bb = 0; bb < 2; ++bb) {
       F ub_prev;
       lw_step_rev(-dflb(0), L.tau[bb], w.flu[1][bb], fb[bb], dfb[bb], L.st0, L.st1, F(-1),
@@ -1167,7 +1177,7 @@ SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow&
     radset_d(c.t[k], F(p.epslw), fb, dfb);
     F tb[4] = {F(0), F(0), F(0), F(0)};
     F s0b = (k == 1) ? st0b_1 : F(0), s1b = F(0);
-    SPD_ROLL
+    SPD_BANDS
     for (int bb = 0; bb < 4; ++bb) {
       F nb;
       lw_step_rev(Ub[bb] + Sb, L.tau[bb], w.flu[k + 1][bb], fb[bb], dfb[bb], L.st0, L.st1,
@@ -1180,7 +1190,7 @@ SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow&
   F fbs[4], dfbs[4];
   radset_d(c.tsfc, F(p.epslw), fbs, dfbs);
   rlus2_b = dflb(KX - 1) * F(p.epslw);
-  SPD_ROLL
+  SPD_BANDS
   for (int bb = 0; bb < 4; ++bb) {
     const F u = Ub[bb] + dflb(KX - 1);
     rlus2_b += u * fbs[bb];
@@ -1199,7 +1209,7 @@ SPD_HD void longwave_rev_down(const Ctx& x, const Col<KX, F>& c, const Lw<KX, F>
   auto dflb = [&](int k) { return dt_b[k] * F(vg.grdscp[k]) / c.psa; };
   const F corlw_b = rlds_b - dflb(KX - 1);
   F Db[4];
-  SPD_ROLL
+  SPD_BANDS
   for (int bb = 0; bb < 4; ++bb) Db[bb] = rlds_b * F(p.emisfc);
   F fb[4], dfb[4];
   LwLevel<F> L;
@@ -1211,8 +1221,9 @@ SPD_HD void longwave_rev_down(const Ctx& x, const Col<KX, F>& c, const Lw<KX, F>
     F tb[4] = {F(0), F(0), F(0), F(0)};
     F s0b = (k == KX - 1) ? corlw_b * (F(p.epslw) * F(p.emisfc)) : F(0), s1b = F(0);
     const int nb_ = (k == 0) ? 2 : 4;
-    SPD_ROLL
-    for (int bb = 0; bb < nb_; ++bb) {
+    SPD_BANDS
+    for (int bb = 0; bb < 4; ++bb) {
+      if (bb >= nb_) continue;
       F nb;
       const F prev = (k == 0) ? F(0) : w.fld[k - 1][bb];
       lw_step_rev(Db[bb] + Sb, L.tau[bb], prev, fb[bb], dfb[bb], L.st0, L.st1, F(1), tb[bb],
@@ -1768,7 +1779,7 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   for (int k = 0; k < KX; ++k)
     b.t[k] = b.q[k] = b.phi[k] = b.qsat[k] = F(0);
   b.psa = b.u = b.v = F(0);
-  SPD_ROLL
+  SPD_BANDS
   for (int j = 0; j < P_N; ++j) b.par[j] = F(0);
   // ---- reverse ----
   vdiff_rev(x, c, dt_b, dq_b, b);
