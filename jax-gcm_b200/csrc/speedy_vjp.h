@@ -24,14 +24,19 @@
 #include "speedy_b200.h"
 #include "speedy_generic.h"
 
-// The per-level loops stay rolled (SPD_ROLL); the loops over the four longwave bands (and the
-// parameter adjoints) are unrolled on the device, so that their small arrays (band fluxes,
-// transmissivities, blackbody fractions and their adjoints) are registers rather than local
-// memory.
+// Loop unrolling on the device: every loop of the reverse pass is unrolled fully (the level
+// count is a template parameter).  Indexed by constants, the small arrays (band fluxes,
+// transmissivities, blackbody fractions and their adjoints) become registers and the per-level
+// arrays are placed by the register allocator, spilled where they must be, instead of all
+// living in local memory behind a dynamic index.  Measured on T170 with 16 levels: 0.916 ms
+// with every loop rolled, 0.777 with the band loops unrolled, level loops unrolled by 2 / 4 / 8
+// 0.748 / 0.728 / 0.701, fully 0.619.
 #if defined(__CUDA_ARCH__)
 #define SPD_BANDS _Pragma("unroll")
+#define SPD_LEVELS _Pragma("unroll")
 #else
 #define SPD_BANDS
+#define SPD_LEVELS
 #endif
 
 namespace spdvjp {
@@ -167,7 +172,7 @@ struct Ctx {
 // ---------------------------------------------------------------------------------------------
 template <int KX, class F>
 SPD_HD void humidity(const Ctx& x, Col<KX, F>& c) {
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     F d_t, d_p;
     c.qsat[k] = qsat_d(c.t[k], c.psa, F(x.vg->fsg[k]), d_t, d_p);
@@ -176,7 +181,7 @@ SPD_HD void humidity(const Ctx& x, Col<KX, F>& c) {
 
 template <int KX, class F>
 SPD_HD void humidity_rev(const Ctx& x, const Col<KX, F>& c, Bar<KX, F>& b) {
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     F d_t, d_p;
     qsat_d(c.t[k], c.psa, F(x.vg->fsg[k]), d_t, d_p);
@@ -202,7 +207,7 @@ SPD_HD void dconv(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c) {
   const F mse1 = vmin(mse0, c.SE(KX - 2) + F(2501.0) * c.q[KX - 2]);
   const F mss0 = vmax(mse0, c.SE(KX - 1) + F(2501.0) * c.qsat[KX - 1]);
   int ktop1 = KX, ktop2 = KX;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 4; k >= 2; --k) {
     const F m2 = mss2_at(x, c, k);
     if (mss0 > m2) ktop1 = k + 1;
@@ -273,21 +278,21 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   const spd_vgrid_t& vg = *x.vg;
   const int iptop = c.iptop_cv;
   w.sentr = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX - 1; ++k) {
     const F e = vmax(F(0), F(vg.fsg[k]) - F(0.5));
     w.entr[k] = e * e;
     w.sentr = w.sentr + w.entr[k];
   }
   w.escale = g.entmax / w.sentr;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX - 1; ++k) w.entr[k] = w.entr[k] * w.escale;
   w.fm0 = F(1e5) * F(vg.dhs[KX - 1]) / (F(9.81) * g.trcnv * F(3600.0));
   w.rdps = F(2.0) / (F(1.0) - g.psmin);
   const bool mask = iptop < KX;
   w.qmax = vmax(F(1.01) * c.q[KX - 1], c.qsat[KX - 1]);
   w.sb3[0] = w.qb3[0] = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     w.sb3[k] = c.SE(k - 1) + F(vg.wvi[k - 1][1]) * (c.SE(k) - c.SE(k - 1));
     w.qb3[k] = c.q[k - 1] + F(vg.wvi[k - 1][1]) * (c.q[k] - c.q[k - 1]);
@@ -305,7 +310,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   w.fds = w.fmass * w.sb;
   w.fdq = w.fmass * w.qb;
   F cm = F(0), cs = F(0), cq = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 0; --k) {
     const bool lm = (k <= KX - 2) && (k >= iptop);
     F en = (k >= 1 && k <= KX - 2) ? w.entr[k] * c.psa * w.cbmf : F(0);
@@ -321,7 +326,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   }
   w.dfse[KX - 1] = w.fds - w.fus;
   w.dfqa[KX - 1] = w.fdq - w.fuq;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX - 1; ++k) {
     const bool lm = (k >= iptop);
     const F a = (w.fus3[k + 1] - w.fds3[k + 1]) - (w.fus3[k] - w.fds3[k]);
@@ -330,7 +335,7 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
     w.dfqa[k] = lm ? bq : F(0) * bq;
   }
   F fsq_sum = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     const bool lm = (k <= KX - 2) && (k >= iptop);
     const F d0 = g.rhil * c.qsat[k] - c.q[k];
@@ -357,7 +362,7 @@ template <int KX, class F>
 SPD_HD void conv_tend(const Ctx& x, const Cv<KX, F>& w, F dt[KX], F dq[KX]) {
   dt[0] = dt[0] + w.dfse[0];
   dq[0] = dq[0] + w.dfqa[0];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     dt[k] = dt[k] + w.dfse[k] * w.rps * F(x.vg->grdscp[k]);
     dq[k] = dq[k] + w.dfqa[k] * w.rps * F(x.vg->grdsig[k]);
@@ -373,7 +378,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   F rps_b = F(0);
   dfse_b[0] = dt_b[0];
   dfqa_b[0] = dq_b[0];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     dfse_b[k] = dt_b[k] * F(vg.grdscp[k]) * w.rps;
     dfqa_b[k] = dq_b[k] * F(vg.grdsig[k]) * w.rps;
@@ -381,7 +386,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   }
   b.psa += -rps_b * (w.rps / c.psa);
   F fus3_b[KX], fuq3_b[KX], fds3_b[KX], fdq3_b[KX], fm3_b[KX], sb3_b[KX], qb3_b[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k)
     fus3_b[k] = fuq3_b[k] = fds3_b[k] = fdq3_b[k] = fm3_b[k] = sb3_b[k] = qb3_b[k] = F(0);
   if (iptop <= KX - 1) {
@@ -404,7 +409,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   // dfqa[KX-1] -= sum(fsq); dfqa[k] += fsq[k]
   const F fsq_sum_b = -dfqa_b[KX - 1];
   F cbmf_b = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     const bool lm = (k <= KX - 2) && (k >= iptop);
     if (!lm) continue;
@@ -420,7 +425,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   }
   F fds_b = dfse_b[KX - 1], fus_b = -dfse_b[KX - 1];
   F fdq_b = dfqa_b[KX - 1], fuq_b = -dfqa_b[KX - 1];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX - 1; ++k) {
     if (k < iptop) continue;
     const F a = dfse_b[k], q = dfqa_b[k];
@@ -435,7 +440,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   }
   // the downward accumulation of entrainment
   F fmass_b = F(0), CMB = F(0), CSB = F(0), CQB = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     if (k == KX - 1) {
       fds_b += fds3_b[k];
@@ -494,7 +499,7 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   qb3_b[KX - 1] += qb_b * wmin(w.qb3[KX - 1], c.q[KX - 1]);
   b.q[KX - 1] += qb_b * wmin(c.q[KX - 1], w.qb3[KX - 1]);
   sb3_b[KX - 1] += sb_b;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F ww = F(vg.wvi[k - 1][1]);
     b.add_se(k - 1, sb3_b[k] - ww * sb3_b[k]);
@@ -524,7 +529,7 @@ SPD_HD void lsc(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, F* dt, F* d
   const F psa2 = c.psa * c.psa;
   F psum = F(0);
   int first = 0;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F sig2 = F(vg.fsg[k]) * F(vg.fsg[k]);
     const F rhref = vmax(g.rhlsc + g.drhlsc * (sig2 - F(1.0)), g.rhblsc);
@@ -556,7 +561,7 @@ SPD_HD void lsc_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, c
   F psum = F(0);
   F rtlsc_b = F(0), psa2_b = F(0);
   // precls = (0 - psum) * psa: psum is needed first
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F sig2 = F(vg.fsg[k]) * F(vg.fsg[k]);
     const F rhref = vmax(g.rhlsc + g.drhlsc * (sig2 - F(1.0)), g.rhblsc);
@@ -565,7 +570,7 @@ SPD_HD void lsc_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, c
   }
   b.psa += precls_b * (F(0) - psum);
   const F psum_b = -precls_b * c.psa;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F sig2 = F(vg.fsg[k]) * F(vg.fsg[k]);
     const F X = g.rhlsc + g.drhlsc * (sig2 - F(1.0));
@@ -615,7 +620,7 @@ SPD_HD void clouds(const Ctx& x, Col<KX, F>& c, Cl<KX, F>& w, F fmask) {
   const int icl0 = w.m0 ? nl1 : KX;
   w.mk = 0u;
   w.cmax = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX - 2; ++k) {
     const F drh = c.RH(k) - F(p.rhcl1);
     const bool m = drh > w.cloudc0 && c.q[k] > F(p.qacl);
@@ -625,7 +630,7 @@ SPD_HD void clouds(const Ctx& x, Col<KX, F>& c, Cl<KX, F>& w, F fmask) {
     w.pm[k] = w.cmax;
   }
   int icl = -1;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX - 2; ++k) {
     const int cand = (w.cmax == w.upd[k]) ? (((w.mk >> k) & 1u) ? k : icl0) : icl0;
     icl = cand > icl ? cand : icl;
@@ -694,7 +699,7 @@ SPD_HD void clouds_rev(const Ctx& x, const Col<KX, F>& c, const Cl<KX, F>& w, F 
   const F rrcl = F(1.0) / (F(p.rhcl2) - F(p.rhcl1));
   F cmax_b = cc_b * wmin(w.cmax * rrcl, F(1.0)) * rrcl;
   F cloudc0_b = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 3; k >= 2; --k) {
     F ub;
     if (k > 2) {
@@ -730,14 +735,14 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
   const spd_vgrid_t& vg = *x.vg;
   const spd_params_t& p = *x.p;
   const bool cmask = c.icltop < KX;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) w.r[k] = (((x.S >> k) & 1u) && cmask) ? g.albcl * c.cloudc : F(0);
   w.r[KX - 1] = g.albcls * c.clstr;
   w.psaz = c.psa * F(z.zenit);
   w.mnq = vmin(F(p.abscl1) * c.qcloud, F(p.abscl2));
   w.acloud = c.cloudc * w.mnq;
   w.tau0[0] = fexp(-w.psaz * F(vg.dhs[0]) * F(p.absdry));
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX - 1; ++k) {
     const F abs1 = F(p.absdry) + F(p.absaer) * (F(vg.fsg[k]) * F(vg.fsg[k]));
     const F cl = (k >= c.icltop) ? w.acloud : F(0) * w.acloud;
@@ -748,7 +753,7 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
     w.tau0[KX - 1] = fexp(-w.psaz * F(vg.dhs[KX - 1]) * (abs1 + F(p.abswv1) * c.q[KX - 1]));
   }
   w.tau1[0] = F(1);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k)
     w.tau1[k] = fexp(-w.psaz * F(vg.dhs[k]) * F(p.abswv2) * c.q[k]);
   F f1 = F(z.fsol) * F(0.95);
@@ -763,7 +768,7 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
   F rs[KX];
   rs[0] = w.r[0];
   rs[1] = w.r[1];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX; ++k) {
     const F prev = f1;
     w.f1v[k] = prev;
@@ -773,7 +778,7 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
   }
   w.f1 = f1;
   F f2 = F(z.fsol) * F(0.05);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F prev = f2;
     w.f2v[k] = prev;
@@ -784,7 +789,7 @@ SPD_HD void shortwave(const Ctx& x, const DiffParams<F>& g, Col<KX, F>& c, const
   F up = f1 * c.albsfc;
   w.upv[KX] = up;
   w.dfabs[KX - 1] = w.dfabs[KX - 1] + up * (F(1) - w.tau0[KX - 1]);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 1; --k) {
     up = up * w.tau0[k] + rs[k];
     w.upv[k] = up;
@@ -803,7 +808,7 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
   const spd_params_t& p = *x.p;
   const bool swon = (x.model_step % 3) == 0;
   F dfabs_b[KX], tau0_b[KX], tau1_b[KX], r_b[KX], rs_b[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     dfabs_b[k] = F(0);
     if (swon) {
@@ -818,7 +823,7 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
   tau0_b[0] += fsw0_b * w.upv[1];
   F up_b = fsw0_b * w.tau0[0];
   r_b[0] += fsw0_b;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     up_b += dfabs_b[k - 1] * (F(1) - w.tau0[k - 1]);
     tau0_b[k - 1] -= dfabs_b[k - 1] * w.upv[k];
@@ -829,14 +834,14 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
   up_b += dfabs_b[KX - 1] * (F(1) - w.tau0[KX - 1]);
   tau0_b[KX - 1] -= dfabs_b[KX - 1] * w.upv[KX];
   f1_b += up_b * c.albsfc;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 1; --k) {
     tau1_b[k] += f2_b * w.f2v[k] - dfabs_b[k] * w.f2v[k];
     f2_b = f2_b * w.tau1[k] + dfabs_b[k] * (F(1) - w.tau1[k]);
   }
   r_b[1] += rs_b[1];
   r_b[0] += rs_b[0];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 2; --k) {
     const F prev = w.f1v[k];
     const F om = F(1) - w.r[k];
@@ -860,7 +865,7 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
     b.psa -= fa_b * w.tau0[0] * F(z.ozupp);
   }
   F psaz_b = F(0), acloud_b = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F Eb = tau1_b[k] * w.tau1[k];
     const F c0 = F(vg.dhs[k]) * F(p.abswv2);
@@ -868,7 +873,7 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
     psaz_b += -Eb * c0 * c.q[k];
   }
   psaz_b += -tau0_b[0] * w.tau0[0] * F(vg.dhs[0]) * F(p.absdry);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F Eb = tau0_b[k] * w.tau0[k];
     const F abs1 = F(p.absdry) + F(p.absaer) * (F(vg.fsg[k]) * F(vg.fsg[k]));
@@ -885,7 +890,7 @@ SPD_HD void shortwave_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>
   b.par[P_ALBCLS] += r_b[KX - 1] * c.clstr;
   clstr_b += r_b[KX - 1] * g.albcls;
   const bool cmask = c.icltop < KX;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX - 1; ++k) {
     if (((x.S >> k) & 1u) && cmask) {
       b.par[P_ALBCL] += r_b[k] * c.cloudc;
@@ -974,7 +979,7 @@ SPD_HD void longwave_down(const Ctx& x, Col<KX, F>& c, F ablco2, Lw<KX, F>& w) {
   F sprev = ((w.fld[0][0] + w.fld[0][1]) + w.fld[0][2]) + w.fld[0][3];
   c.dfl[0] = F(0) + (-sprev);
   F st0_last = L.st0;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
@@ -1010,7 +1015,7 @@ SPD_HD void longwave_up(const Ctx& x, Col<KX, F>& c, const SurfaceRow& z, F ablc
   for (int b = 0; b < 4; ++b) w.flu[KX][b] = fb[b] * c.rlus2 + refsfc * fsw[b];
   c.dfl[KX - 1] = c.dfl[KX - 1] + F(p.epslw) * c.rlus2;
   F sk = ((w.flu[KX][0] + w.flu[KX][1]) + w.flu[KX][2]) + w.flu[KX][3];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 1; --k) {
     lw_level(x, c, k, ablco2, L);
     radset_d(c.t[k], F(p.epslw), fb, dfb);
@@ -1138,7 +1143,7 @@ SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow&
   const spd_vgrid_t& vg = *x.vg;
   const spd_params_t& p = *x.p;
   auto dflb = [&](int k) { return dt_b[k] * F(vg.grdscp[k]) / c.psa; };
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) b.psa += -dt_b[k] * ((c.dfl[k] * F(vg.grdscp[k])) / c.psa) / c.psa;
   F st0b_0, st0b_1;
   {
@@ -1170,7 +1175,7 @@ SPD_HD void longwave_rev_up(const Ctx& x, const Col<KX, F>& c, const SurfaceRow&
     }
     lw_level_rev(x, c, 0, ablco2, L, tb, s0b, s1b, acl1_b, acl2_b, b);
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 1; k < KX; ++k) {
     const F Sb = (k >= 2 ? dflb(k - 1) : F(0)) - dflb(k);
     lw_level(x, c, k, ablco2, L);
@@ -1213,7 +1218,7 @@ SPD_HD void longwave_rev_down(const Ctx& x, const Col<KX, F>& c, const Lw<KX, F>
   for (int bb = 0; bb < 4; ++bb) Db[bb] = rlds_b * F(p.emisfc);
   F fb[4], dfb[4];
   LwLevel<F> L;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = KX - 1; k >= 0; --k) {
     const F Sb = -dflb(k) + (k < KX - 1 ? dflb(k + 1) : F(0));
     lw_level(x, c, k, ablco2, L);
@@ -1573,7 +1578,7 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
   const int nl1 = KX - 1;
   const int icnv = KX - c.iptop - 1;
   F tt[KX], qt[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) tt[k] = qt[k] = F(0);
   const F dmse = c.SE(KX - 1) - c.SE(nl1 - 1) + F(2501.0) * (c.q[KX - 1] - c.qsat[nl1 - 1]);
   const F drh = c.RH(KX - 1) - c.RH(nl1 - 1);
@@ -1593,7 +1598,7 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
     qt[KX - 1] = -fq * (F(1) / F(vg.dhs[KX - 1]));
   }
   F fluxq[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX - 2; ++k) {
     const bool cond = F(vg.hsg[k + 1]) > F(0.5);
     const F d0 = F(p.rhgrad) * (F(vg.fsg[k + 1]) - F(vg.fsg[k]));
@@ -1602,22 +1607,22 @@ SPD_HD void vdiff(const Ctx& x, const Col<KX, F>& c, F* dt, F* dq) {
     fluxq[k] = (dr >= d0 && cond) ? f2 * c.qsat[k] * dr : F(0);
     qt[k] = qt[k] + fluxq[k] * (F(1) / F(vg.dhs[k]));
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX - 2; ++k) qt[k + 1] = qt[k + 1] + (-fluxq[k] * (F(1) / F(vg.dhs[k + 1])));
   F fse[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < nl1; ++k) {
     const F se0 = c.SE(k + 1) - F(p.segrad) * (c.phi[k + 1] - c.phi[k]);
     fse[k] = (c.SE(k) < se0) ? v.fvdise * (se0 - c.SE(k)) : F(0);
     tt[k] = tt[k] + fse[k] * (F(1) / F(vg.dhs[k]));
   }
   F cum = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < nl1; ++k) {
     cum = cum + fse[k] * (F(1) / (F(1) - F(vg.hsg[k + 1])));
     tt[k + 1] = tt[k + 1] + (-cum);
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     dt[k] = dt[k] + tt[k];
     dq[k] = dq[k] + qt[k];
@@ -1634,7 +1639,7 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
   const int icnv = KX - c.iptop - 1;
   // the cumulative flux: tt[k+1] -= sum_{j<=k} fse[j] / (1 - hsg[j+1])
   F acc = F(0);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = nl1 - 1; k >= 0; --k) {
     acc += -dt_b[k + 1];
     const F fse_b = acc * (F(1) / (F(1) - F(vg.hsg[k + 1]))) + dt_b[k] * (F(1) / F(vg.dhs[k]));
@@ -1647,7 +1652,7 @@ SPD_HD void vdiff_rev(const Ctx& x, const Col<KX, F>& c, const F* dt_b, const F*
       b.phi[k] += s_b * F(p.segrad);
     }
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 2; k < KX - 2; ++k) {
     const bool cond = F(vg.hsg[k + 1]) > F(0.5);
     const F d0 = F(p.rhgrad) * (F(vg.fsg[k + 1]) - F(vg.fsg[k]));
@@ -1704,7 +1709,7 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   const spd_params_t& p = *x.p;
   const bool verify = (x.flags & SPD_FUSE_VERIFY) != 0;
   Col<KX, F> c;
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     c.t[k] = in.t[k];
     c.q[k] = (verify && in.q[k] < F(0)) ? F(0) : in.q[k];
@@ -1727,7 +1732,7 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   }
   // ---- forward ----
   F dq[KX], dt[KX];
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) dq[k] = dt[k] = F(0);
   humidity(x, c);
   dconv(x, g, c);
@@ -1762,11 +1767,11 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
     vdiff(x, c, dt, dq);
     if (qcorv && (x.flags & SPD_OROGRAPHIC)) {  // the last term's humidity tendency
       const F qcorh = orographic_qcorh(in.phis0, in.fmask, in.stl, in.sst, F(gamlat), F(pexp));
-      SPD_ROLL
+      SPD_LEVELS
       for (int k = 0; k < KX; ++k) dq[k] = dq[k] + (qcorh * F(qcorv[k])) / dt_seconds;
     }
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     F qb = ct_q[k] * q_tend_scale;
     if (verify && !(in.q[k] + dt_seconds * dq[k] >= F(0))) {
@@ -1775,7 +1780,7 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
     }
     dq_b[k] = qb;
   }
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k)
     b.t[k] = b.q[k] = b.phi[k] = b.qsat[k] = F(0);
   b.psa = b.u = b.v = F(0);
@@ -1804,7 +1809,7 @@ SPD_HD void column_vjp(const Ctx& x, const DiffParams<F>& g, F ablco2, F dt_seco
   const F qdif_b = conv_rev(x, g, c, sc.cv, dt_b, dq_b, precnv_b, b);
   dconv_rev(x, g, c, qdif_b, b);
   humidity_rev(x, c, b);
-  SPD_ROLL
+  SPD_LEVELS
   for (int k = 0; k < KX; ++k) {
     const F qb = (verify && in.q[k] < F(0)) ? F(0) : b.q[k];
     b.q[k] = qb + (((limited >> k) & 1u) ? -(ct_q[k] * q_tend_scale) / dt_seconds : F(0));
