@@ -36,8 +36,10 @@ sys.path.insert(0, ROOT)
 NCU_TRAFFIC_PER_COLUMN = {"ensemble": (179.059968e6 + 49.081344e6) / 466944,
                           "t425": (370.422016e6 + 155.600640e6) / 819200}
 # Warp instructions per launch of the dominant kernel (smsp__inst_executed.sum, same captures):
-# the compute side of the roofline, against one instruction per scheduler per cycle.
-NCU_WARP_INSTRUCTIONS = {"ensemble": 91634472.0, "t425": 195374955.0}
+# the compute side of the roofline, against one instruction per scheduler per cycle.  The
+# adjoint's is ensemble_adjoint at T170 with 16 levels (profiles/ensemble_adjoint_t170.md).
+NCU_WARP_INSTRUCTIONS = {"ensemble": 91634472.0, "t425": 195374955.0,
+                         "adjoint_t170": 117031373.0}
 
 
 def parse_args():
@@ -384,7 +386,8 @@ def run_b200(args):
             sections["t425"] = t425_section(pkg, dev, peak, peak_kind,
                                             clk["sm_mhz"] if clk else None)
         if "adjoint" in wanted:
-            sections["adjoint"] = adjoint_section(pkg, dev)
+            sections["adjoint"] = adjoint_section(pkg, dev, peak, peak_kind,
+                                                  clk["sm_mhz"] if clk else None)
         if "serving" in wanted:
             sections["serving"] = serving_section(pkg, dev, args.serving_requests)
         if "held_suarez" in wanted:
@@ -520,9 +523,10 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
     return out_d
 
 
-def adjoint_section(pkg, dev):
+def adjoint_section(pkg, dev, peak=None, peak_kind=None, sm_mhz=None):
     """Adjoint at T42 (128x64 = 8,192 columns, 8 levels): one VJP call beside one forward call,
-    and the 48-step rollout VJP with checkpoints every 8 steps; plus the VJP at T170x16."""
+    and the 48-step rollout VJP with checkpoints every 8 steps; plus the VJP at T170x16 with
+    its place against HBM (B_vjp = 4 (10 kx + 15) bytes per column) and instruction issue."""
     import torch
     res = {}
     for label, (ix, il, kx) in (("t42_k8", (128, 64, 8)), ("t170_k16", (512, 256, 16))):
@@ -543,6 +547,16 @@ def adjoint_section(pkg, dev):
                                2, warmup=1)
             r["rollout48_vjp_ms"] = round(roll_ms, 2)
             r["rollout48_checkpoint_every"] = 8
+        else:
+            nbytes = 4 * (10 * kx + 15) * inst.columns
+            r["algorithmic_bytes"] = nbytes
+            if peak:
+                r["hbm_frac_of_call"] = round(nbytes / (vjp_ms / 1e3) / 1e9 / peak, 4)
+                r["peak_kind"] = peak_kind
+            if sm_mhz:
+                sms = torch.cuda.get_device_properties(dev).multi_processor_count
+                ach = NCU_WARP_INSTRUCTIONS["adjoint_t170"] / (vjp_ms / 1e3)
+                r["issue_frac_of_call"] = round(ach / (sms * 4 * sm_mhz * 1e6), 4)
         res[label] = r
     return res
 
