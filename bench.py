@@ -319,7 +319,7 @@ def run_b200(args):
                 pipe.submit()
             pipe.end()
 
-        pipe_steps(2)
+        pipe_steps(max(3, args.warmup))
         torch.cuda.synchronize()
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -364,7 +364,8 @@ def run_b200(args):
                     v.copy_(out[k], non_blocking=True)
             torch.cuda.current_stream().synchronize()
 
-        e2e_ms = timed(e2e_step, max(3, args.steps // 2), 2) / max(3, args.steps // 2)
+        e2e_ms = (timed(e2e_step, max(3, args.steps // 2), max(3, args.warmup)) /
+                  max(3, args.steps // 2))
     if not args.no_e2e:
         e2e = {"value": cols * world / (e2e_ms / 1e3), "unit": "columns/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -490,7 +491,7 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
     with torch.cuda.graph(g):
         for _ in range(24):
             call()
-    graph_ms = event_ms(g.replay, 5, warmup=2) / 24
+    graph_ms = event_ms(g.replay, 5, warmup=3) / 24
     cols = inst.columns
     nbytes = pkg.synthetic.fwd_bytes(inst.kx, cols)
     b2 = pkg.synthetic.second_half_bytes(inst.kx, cols)
@@ -544,7 +545,7 @@ def adjoint_section(pkg, dev, peak=None, peak_kind=None, sm_mhz=None):
         if label == "t42_k8":
             roll_ms = event_ms(lambda: pkg.rollout.rollout_vjp(None, st, fo, ge, da, ct,
                                                                nsteps=48, checkpoint_every=8),
-                               2, warmup=1)
+                               2, warmup=3)
             r["rollout48_vjp_ms"] = round(roll_ms, 2)
             r["rollout48_checkpoint_every"] = 8
         else:
