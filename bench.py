@@ -30,15 +30,15 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per column of the dominant kernel's launch (the second launch,
 # ensemble_columns), from one ncu capture each (profiles/ensemble_columns_ragged_ensemble.md:
-# 179.1 MB read + 49.1 MB written over 466,944 columns; profiles/ensemble_columns_t425.md:
-# 370.4 + 155.6 MB over 819,200 columns).  Part of each launch's writes is still in L2 when the
+# 179.1 MB read + 48.4 MB written over 466,944 columns; profiles/ensemble_columns_t425.md:
+# 370.4 + 156.4 MB over 819,200 columns).  Part of each launch's writes is still in L2 when the
 # kernel ends, so the write share reads low.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": (179.059968e6 + 49.081344e6) / 466944,
-                          "t425": (370.422016e6 + 155.600640e6) / 819200}
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": (179.083264e6 + 48.404224e6) / 466944,
+                          "t425": (370.373120e6 + 156.422400e6) / 819200}
 # Warp instructions per launch of the dominant kernel (smsp__inst_executed.sum, same captures):
 # the compute side of the roofline, against one instruction per scheduler per cycle.  The
 # adjoint's is ensemble_adjoint at T170 with 16 levels (profiles/ensemble_adjoint_t170.md).
-NCU_WARP_INSTRUCTIONS = {"ensemble": 91634472.0, "t425": 195374955.0,
+NCU_WARP_INSTRUCTIONS = {"ensemble": 80446120.0, "t425": 170901355.0,
                          "adjoint_t170": 117031373.0}
 
 
