@@ -73,6 +73,83 @@ def test_plan_rejects_bad_class(pkg):
     assert rc == 2
 
 
+CT_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity")
+GRAD_FIELDS = ("u_wind", "v_wind", "temperature", "specific_humidity", "geopotential",
+               "normalized_surface_pressure", "params")
+
+
+def _fake_vjp_member(L, ix, il, cls, slot):
+    m = L.VjpMember()
+    m.inp, _ = fake_fields(L)  # never dereferenced by the plan
+    base = (1 << 40) + slot * (1 << 34)
+    m.ct = L.Cotangents(**{k: base + i * (1 << 28) for i, k in enumerate(CT_FIELDS)})
+    m.grads = L.Grads(**{k: base + (4 + i) * (1 << 28) for i, k in enumerate(GRAD_FIELDS)})
+    m.ix, m.il, m.cls = ix, il, cls
+    return m
+
+
+def test_vjp_plan_layout_tiles_and_records(pkg):
+    """The adjoint's plan (host side): every column once, 16-level members first, and each
+    member record carrying its column count, level count, class, level-set word and table."""
+    L = pkg._lib
+    lib = L.load()
+    classes = (L.Class * 2)()
+    classes[0].desc.kx, classes[1].desc.kx = 8, 16
+    shapes = [(64, 32, 0), (96, 48, 1), (64, 32, 1), (7, 3, 0)]
+    mem = (L.VjpMember * len(shapes))(*[_fake_vjp_member(L, *s, i)
+                                        for i, s in enumerate(shapes)])
+    n = lib.spd_ensemble_vjp_plan_bytes(mem, len(shapes))
+    host = (C.c_ubyte * n)()
+    info = L.PlanInfo()
+    dev_base = 1 << 32
+    rc = lib.spd_ensemble_vjp_plan(classes, 2, mem, len(shapes), C.cast(host, C.c_void_p),
+                                   C.c_void_p(dev_base), n, C.byref(info))
+    assert rc == 0
+    assert info.ntiles == sum((ix * il + 127) // 128 for ix, il, _ in shapes)
+    raw = bytes(host)
+    head = C.sizeof(L.Inputs) + C.sizeof(L.Cotangents) + C.sizeof(L.Grads)
+    msize = head + 4 * 4 + 2 * 8
+    kx_of = [8, 16, 16, 8]
+    tables = set()
+    for i, (ix, il, cls) in enumerate(shapes):
+        rec = 256 + i * msize
+        cols, il_, kx, cls_ = np.frombuffer(raw, np.int32, 4, rec + head)
+        assert (cols, il_, kx, cls_) == (ix * il, il, kx_of[i], cls)
+        s_ptr, table = np.frombuffer(raw, np.uint64, 2, rec + head + 16)
+        assert s_ptr == dev_base + info.levelset_offset + 4 * i
+        tables.add(int(table))
+    assert len(tables) == len(shapes) and all(t % 256 == 0 for t in tables)
+    tiles_off = 256 + ((len(shapes) * msize + 255) // 256) * 256
+    tiles = np.frombuffer(raw, np.int32, 2 * info.ntiles, tiles_off).reshape(-1, 2)
+    order = [kx_of[m] for m in tiles[:, 0]]
+    assert order == sorted(order, reverse=True)
+    covered = {}
+    for m, c0 in tiles:
+        covered.setdefault(int(m), []).append(int(c0))
+    for i, (ix, il, _) in enumerate(shapes):
+        assert covered[i] == list(range(0, ix * il, 128))
+
+
+def test_vjp_plan_rejects_missing_cotangent_and_bad_class(pkg):
+    L = pkg._lib
+    lib = L.load()
+    classes = (L.Class * 1)()
+    classes[0].desc.kx = 8
+
+    def plan(m):
+        mem = (L.VjpMember * 1)(m)
+        n = lib.spd_ensemble_vjp_plan_bytes(mem, 1)
+        host = (C.c_ubyte * n)()
+        return lib.spd_ensemble_vjp_plan(classes, 1, mem, 1, C.cast(host, C.c_void_p),
+                                         C.c_void_p(1 << 32), n, C.byref(L.PlanInfo()))
+
+    m = _fake_vjp_member(L, 64, 32, 0, 0)
+    assert plan(m) == 0
+    m.ct.temperature = None
+    assert plan(m) == 1
+    assert plan(_fake_vjp_member(L, 64, 32, 2, 0)) == 2
+
+
 def _members(pkg, device):
     insts = [pkg.synthetic.land_instance(500 + i, ix, il, kx)
              for i, (ix, il, kx) in enumerate([(64, 32, 8), (64, 32, 16), (96, 48, 16),
