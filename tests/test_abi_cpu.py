@@ -116,6 +116,38 @@ def test_overlapping_outputs_are_rejected(pkg, lib):
     assert lib.spd_status_string(9).decode().startswith("an output field overlaps")
 
 
+def test_vjp_argument_validation_needs_no_gpu(pkg, lib):
+    """spd_vjp's checks, in order: null arguments, the instance and its cotangent and gradient
+    planes, the scratch (present, 256-byte aligned, large enough), the level count.  Every call
+    here fails a check, so no device work is attempted on the fake addresses."""
+    L = pkg._lib
+    d = L.Desc(8, 16, 8, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    vg, pr = L.VGrid(), L.Params()
+    inp, _ = fake_fields(L)
+    base = 1 << 40
+    cts = ("u_wind", "v_wind", "temperature", "specific_humidity")
+    grs = cts + ("geopotential", "normalized_surface_pressure", "params")
+    ct = L.Cotangents(**{k: base + i * (1 << 28) for i, k in enumerate(cts)})
+    gr = L.Grads(**{k: base + (4 + i) * (1 << 28) for i, k in enumerate(grs)})
+    n = lib.spd_vjp_scratch_bytes(C.byref(d))
+    assert n > 0 and n % 256 == 0
+
+    def call(desc, scratch, nbytes):
+        return lib.spd_vjp(C.byref(desc) if desc is not None else None, C.byref(vg),
+                           C.byref(pr), C.byref(inp), C.byref(ct), C.byref(gr),
+                           C.c_void_p(scratch) if scratch else None, nbytes, None)
+
+    assert call(None, 1 << 32, n) == 1
+    assert call(d, None, n) == 4
+    assert call(d, (1 << 32) + 16, n) == 4      # misaligned
+    assert call(d, 1 << 32, n - 256) == 4       # too small
+    d.kx = 9
+    assert call(d, 1 << 32, n) == 3
+    d.kx = 8
+    ct.temperature = None
+    assert call(d, 1 << 32, n) == 1
+
+
 def test_product_path_fails_loudly_without_library(pkg, monkeypatch):
     monkeypatch.setattr(pkg._lib, "_lib", None)
     monkeypatch.setattr(pkg._lib, "LIB_PATH", "/nonexistent/libspeedy_b200.so")
