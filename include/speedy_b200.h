@@ -44,7 +44,9 @@ enum spd_status {
   SPD_ERR_DEVICE = 6,    /* the device reported an error status (bounded wait expired, ...) */
   SPD_ERR_ALIGN = 7,     /* a field pointer is not 16-byte aligned */
   SPD_ERR_NOALLOC_LIMIT = 8, /* il above SPD_NOALLOC_MAX_IL for spd_fwd_noalloc */
-  SPD_ERR_ALIAS = 9          /* an output field overlaps an input field or another output */
+  SPD_ERR_ALIAS = 9,         /* an output field overlaps an input field or another output */
+  SPD_ERR_STREAM_DEVICE = 10 /* spd_fwd_noalloc: the stream belongs to another device than the
+                                current one */
 };
 
 /* spd_desc_t.flags */
@@ -319,8 +321,12 @@ int spd_ensemble_vjp(const spd_class_t* classes, int nclasses, void* plan_device
 /* no allocation: the scratch lives in a fixed device array of the library (65,792 bytes on   */
 /* every GPU that loads it, kept until process exit), which limits instances to                */
 /* il <= SPD_NOALLOC_MAX_IL latitudes (SPD_ERR_NOALLOC_LIMIT otherwise).                      */
-/*  - The first call on a device looks up the array's device address with that device         */
-/*    current; make that first call before any stream capture.                                */
+/*  - Every call looks up the array's device address in the current device's context          */
+/*    (cudaGetSymbolAddress), so the address never outlives its context (cudaDeviceReset      */
+/*    included).  The first call on a device also loads the library's kernels there; make     */
+/*    that first call before any stream capture.                                              */
+/*  - The stream must belong to the current device (SPD_ERR_STREAM_DEVICE otherwise): the     */
+/*    array used is the current device's.                                                     */
 /*  - Every call uses the same array and clears its level-set word itself.  Calls whose work   */
 /*    overlaps on the GPU (other streams, other host threads) race on the array and corrupt    */
 /*    each other's results: order them, for example on one stream.                            */

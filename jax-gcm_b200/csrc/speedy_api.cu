@@ -193,6 +193,8 @@ const char* spd_status_string(int status) {
       return "instance has more latitudes than spd_fwd_noalloc's fixed scratch holds "
              "(SPD_NOALLOC_MAX_IL)";
     case SPD_ERR_ALIAS: return "an output field overlaps an input field or another output";
+    case SPD_ERR_STREAM_DEVICE:
+      return "the stream belongs to another device than the current one (spd_fwd_noalloc)";
     default: return "unknown status";
   }
 }

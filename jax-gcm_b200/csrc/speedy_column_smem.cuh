@@ -39,6 +39,17 @@ namespace spd {
 
 constexpr int kNT = 128;  // threads per block = columns per block
 
+// Exponential of the second half's transmissivities and drag factor: the hardware exponential
+// __expf; a build with SPD_IEEE_EXP defined uses expf instead (to measure what the hardware
+// exponential changes in the results).
+__device__ __forceinline__ float texp(float x) {
+#ifdef SPD_IEEE_EXP
+  return expf(x);
+#else
+  return __expf(x);
+#endif
+}
+
 // Per-thread level array: element k of this thread lives at p[k * kNT].
 struct Lv {
   float* p;
@@ -351,9 +362,9 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
     const bool gate = (K.model_step % 3) == 0;
     // band-1 transmissivity of level k (lines 80-94)
     auto tau0_at = [&](int k) {
-      if (k == 0) return __expf(-psaz * vg.dhs[0] * p.absdry);
+      if (k == 0) return texp(-psaz * vg.dhs[0] * p.absdry);
       const float cl = (k >= icltop && k < KX - 1) ? acloud : 0.0f;
-      return __expf(-psaz * vg.dhs[k] * (D.abs1[k] + p.abswv1 * Q[k] + cl));
+      return texp(-psaz * vg.dhs[k] * (D.abs1[k] + p.abswv1 * Q[k] + cl));
     };
     auto add_sw = [&](int k, float d) { DT[k] = DT[k] + (gate ? d * vg.grdscp[k] * rps : 0.0f); };
 #pragma unroll 4
@@ -369,7 +380,7 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
     const float d1_band1 = d0 + (-f1);
     float f2 = z.fsol * fband2;
     {  // band 2 at level 1 completes level 1's downward absorption
-      const float tau1 = __expf(-psaz * vg.dhs[1] * p.abswv2 * Q[1]);
+      const float tau1 = texp(-psaz * vg.dhs[1] * p.abswv2 * Q[1]);
       const float prev = f2;
       f2 = prev * tau1;
       add_sw(1, d1_band1);
@@ -381,7 +392,7 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       f1 = prev * t0 * (1.0f - r);
       const float d = prev * (1.0f - r) * (1.0f - t0);
       W[k] = r * prev;
-      const float tau1 = __expf(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
+      const float tau1 = texp(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
       const float prev2 = f2;
       f2 = prev2 * tau1;
       add_sw(k, d);
@@ -419,10 +430,10 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       a2 = fmaxf(a2, acl2);
       a3 = fmaxf(a3, acl2);
     }
-    tau[0] = __expf(-a0 * psa * vg.dhs[k]);
-    tau[1] = __expf(-D.ablco2 * psa * vg.dhs[k]);
-    tau[2] = __expf(-a2 * psa * vg.dhs[k]);
-    tau[3] = __expf(-a3 * psa * vg.dhs[k]);
+    tau[0] = texp(-a0 * psa * vg.dhs[k]);
+    tau[1] = texp(-D.ablco2 * psa * vg.dhs[k]);
+    tau[2] = texp(-a2 * psa * vg.dhs[k]);
+    tau[3] = texp(-a3 * psa * vg.dhs[k]);
   };
   auto add_lw = [&](int k, float d) { DT[k] = DT[k] + d * vg.grdscp[k] * rps; };
 
@@ -496,7 +507,7 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       const float dthl = (tskin > t2_0) ? fminf(p.dtheta, tskin - t2_0)
                                         : fmaxf(-p.dtheta, D.astab * (tskin - t2_0));
       const float denv1 = denv0 * (1.0f + dthl * D.rdth);
-      const float forog = 1.0f + D.rhdrag * (1.0f - __expf(-fmaxf(s.phis0, 0.0f) * D.rhdrag));
+      const float forog = 1.0f + D.rhdrag * (1.0f - texp(-fmaxf(s.phis0, 0.0f) * D.rhdrag));
       const float cdldv = p.cdl * denv0 * forog;
       ustr0 = -cdldv * ua;
       vstr0 = -cdldv * va;

@@ -10,8 +10,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "speedy_column_smem.cuh"
 
 namespace spd {
@@ -29,25 +27,27 @@ constexpr size_t kNoallocHeader = 256;  // level-set word, status word, padding
 constexpr size_t kNoallocBytes = kNoallocHeader + (size_t)SPD_NOALLOC_MAX_IL * sizeof(spd::ZonalRow);
 
 // The shared scratch.  In host code this name is only a host-side stand-in for the symbol;
-// its device address comes from cudaGetSymbolAddress (below), once per device.
+// its device address comes from cudaGetSymbolAddress (below).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_dev_ptr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device (looked up on first use).
+// Device address of g_noalloc_scratch in the current device's context.  It is looked up on
+// every call (after the first call on a device, which loads the module, this is a table lookup
+// in the runtime), so no address outlives the context it belongs to: after cudaDeviceReset or
+// any other teardown of the primary context, the next call gets the new context's address.
 int scratch_address(void** out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SPD_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_dev_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SPD_ERR_CUDA;
-    g_dev_ptr[dev] = p;
-  }
-  *out = g_dev_ptr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return SPD_ERR_CUDA;
+  *out = p;
   return SPD_OK;
+}
+
+// The array exists once per device, so the call must run on the device whose array it uses:
+// the stream's device must be the current device.
+int check_stream_device(cudaStream_t st) {
+  int cur = -1, sdev = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) return SPD_ERR_CUDA;
+  if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) return SPD_ERR_CUDA;
+  return sdev == cur ? SPD_OK : SPD_ERR_STREAM_DEVICE;
 }
 
 }  // namespace
@@ -59,10 +59,12 @@ extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
   if (rc != SPD_OK) return rc;
   if (!vgrid || !params) return SPD_ERR_NULL;
   if (desc->il > SPD_NOALLOC_MAX_IL) return SPD_ERR_NOALLOC_LIMIT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  rc = check_stream_device(st);
+  if (rc != SPD_OK) return rc;
   void* scratch = nullptr;
   rc = scratch_address(&scratch);
   if (rc != SPD_OK) return rc;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   spd::ConstsD CD;
   CD.K = spd::make_consts(desc, vgrid, params);
   CD.D = spd::derive_constants(desc, vgrid, params);

@@ -769,6 +769,11 @@ class CudaBackend:
         return dm
 
     def release(self, dm):
+        # The member's upload may still be running on the copy stream (a prefetched member, or
+        # one left over by an admission that failed part way): the range must not go to
+        # another request's outputs, which a compute stream writes, before that copy ends.
+        if dm.ready is not None:
+            dm.ready.synchronize()
         self.arena.release(dm.handle)
         dm.buf = None
 

@@ -56,6 +56,46 @@ SIGMA_LAYER_BOUNDARIES = {
 }
 
 
+# ---------------------------------------------------------------------------------------------
+# Exponential hook.  Every exp of the physics goes through exp_.  By default it is np.exp.
+# Inside ``perturbed_exp`` each float32 result is multiplied by (1 + r 2^-23), with r drawn
+# uniformly from (-ulps, ulps) per element.  Library exps differ from one another in their last
+# bits, and this is Monte Carlo arithmetic (D. Stott Parker, 1997) applied to the one operation
+# whose rounding differs between float32 implementations.  Re-running the float32 oracle under it
+# measures, per output element, how far last-bit differences in the transcendentals move that
+# element.  The parity tests use this to tell float32 noise from a wrong result.
+# ---------------------------------------------------------------------------------------------
+_EXP_NOISE = None  # (numpy Generator, ulps) while perturbed_exp is active
+
+
+def exp_(x):
+    y = np.exp(x)
+    if _EXP_NOISE is None or np.asarray(y).dtype != np.float32:
+        return y
+    rng, ulps = _EXP_NOISE
+    ya = np.asarray(y)
+    r = rng.uniform(-ulps, ulps, ya.shape)
+    z = (ya.astype(np.float64) * (1.0 + r * 2.0 ** -23)).astype(np.float32)
+    return z if isinstance(y, np.ndarray) else np.float32(z)
+
+
+class perturbed_exp:
+    """Context manager: float32 exp results carry a seeded relative noise of up to ``ulps``."""
+
+    def __init__(self, seed, ulps=2.0):
+        self.noise = (np.random.default_rng(seed), float(ulps))
+
+    def __enter__(self):
+        global _EXP_NOISE
+        self.prev, _EXP_NOISE = _EXP_NOISE, self.noise
+        return self
+
+    def __exit__(self, *exc):
+        global _EXP_NOISE
+        _EXP_NOISE = self.prev
+        return False
+
+
 def ns(**kw):
     return SimpleNamespace(**kw)
 
@@ -281,8 +321,8 @@ def get_qsat(ta, ps, sig, rec=None):
     t2 = 7.66
     with np.errstate(all="ignore"):
         _rec(rec, ta, t0)
-        qsat = np.where(ta >= t0, e0 * np.exp(c1 * (ta - t0) / (ta - t1)),
-                        e0 * np.exp(c2 * (ta - t0) / (ta - t2)))
+        qsat = np.where(ta >= t0, e0 * exp_(c1 * (ta - t0) / (ta - t1)),
+                        e0 * exp_(c2 * (ta - t0) / (ta - t2)))
         qsat = 622.0 * qsat / (sig * ps - 0.378 * qsat)
     return qsat
 
@@ -562,7 +602,7 @@ def set_forcing(state, data, params, forcing, geometry, rec=None):
     albsfc = alb_s + fmask * (alb_l - alb_s)
     iyear_ref = params.forcing.co2_year_ref
     inc = 1.0 if params.forcing.increase_co2 else 0.0
-    ablco2 = ABLCO2_REF * np.exp(inc * DEL_CO2 * (dtype(model_year) + tyear - iyear_ref))
+    ablco2 = ABLCO2_REF * exp_(inc * DEL_CO2 * (dtype(model_year) + tyear - iyear_ref))
     data.mod_radcon.snowc = snowc
     data.mod_radcon.alb_l = alb_l
     data.mod_radcon.alb_s = alb_s
@@ -667,14 +707,14 @@ def shortwave_rad_fluxes(state, data, params, forcing, geometry, rec=None,
     tau2[kx - 1, :, :, 2] = ps.albcls * clstr
     psaz = psa * sw.zenit
     acloud = cloudc * np.minimum(ps.abscl1 * sw.qcloud, ps.abscl2)
-    tau2[0, :, :, 0] = np.exp(-psaz * dhs[0] * ps.absdry)
+    tau2[0, :, :, 0] = exp_(-psaz * dhs[0] * ps.absdry)
     abs1 = ps.absdry + ps.absaer * fsg[1:nl1] ** 2
     cloudy = np.arange(1, nl1)[:, None, None] >= icltop
-    tau2[1:nl1, :, :, 0] = np.exp(-psaz * dhs[1:nl1, None, None] * (
+    tau2[1:nl1, :, :, 0] = exp_(-psaz * dhs[1:nl1, None, None] * (
         abs1[:, None, None] + ps.abswv1 * qa[1:nl1] + cloudy * acloud))
     abs1 = ps.absdry + ps.absaer * fsg[kx - 1] ** 2
-    tau2[kx - 1, :, :, 0] = np.exp(-psaz * dhs[kx - 1] * (abs1 + ps.abswv1 * qa[kx - 1]))
-    tau2[1:kx, :, :, 1] = np.exp(-psaz * dhs[1:kx, None, None] * ps.abswv2 * qa[1:kx])
+    tau2[kx - 1, :, :, 0] = exp_(-psaz * dhs[kx - 1] * (abs1 + ps.abswv1 * qa[kx - 1]))
+    tau2[1:kx, :, :, 1] = exp_(-psaz * dhs[1:kx, None, None] * ps.abswv2 * qa[1:kx])
     dfabs = np.zeros((kx, ix, il), dt_)
     ftop = sw.fsol
     flux_1 = np.zeros((kx, ix, il), dt_)
@@ -721,7 +761,7 @@ def shortwave_rad_fluxes(state, data, params, forcing, geometry, rec=None,
         np.arange(2, kx - 1)[:, None, None] > icltop, acloud1, acloud2)
     absorptivity[2:kx - 1, :, :, 2:] = np.maximum(absorptivity[2:kx - 1, :, :, 2:],
                                                   acloud2[None, :, :, None])
-    tau2 = np.exp(-absorptivity * psa[:, :, None] * dhs[:, None, None, None])
+    tau2 = exp_(-absorptivity * psa[:, :, None] * dhs[:, None, None, None])
     eps1 = params.mod_radcon.epslw / (dhs[0] + dhs[1])
     stratc = np.zeros((ix, il, 2), dt_)
     stratc[:, :, 0] = sw.stratz * psa
@@ -856,7 +896,7 @@ def get_upward_longwave_rad_fluxes(state, data, params, forcing, geometry, rec=N
 def get_orog_land_sfc_drag(phis0, hdrag):
     """get_orog_land_sfc_drag (surface_flux.py:302-315)."""
     rhdrag = 1 / (GRAV * hdrag)
-    return 1.0 + rhdrag * (1.0 - np.exp(-np.maximum(phis0, 0.0) * rhdrag))
+    return 1.0 + rhdrag * (1.0 - exp_(-np.maximum(phis0, 0.0) * rhdrag))
 
 
 def get_surface_fluxes(state, data, params, forcing, geometry, rec=None):
@@ -1104,8 +1144,8 @@ def orographic_horizontal(phis0, fmask, stl, sst):
         psfc = (tsfc / tref) ** pexp
 
         def esat(ta):
-            return np.where(ta >= 273.16, 6.108e-3 * np.exp(17.269 * (ta - 273.16) / (ta - 35.86)),
-                            6.108e-3 * np.exp(21.875 * (ta - 273.16) / (ta - 7.66)))
+            return np.where(ta >= 273.16, 6.108e-3 * exp_(17.269 * (ta - 273.16) / (ta - 35.86)),
+                            6.108e-3 * exp_(21.875 * (ta - 273.16) / (ta - 7.66)))
         e_ref = esat(tref)
         qref = 622.0 * e_ref / (dt_(1.0) - 0.378 * e_ref)
         qsfc = get_qsat(tsfc, psfc, dt_(1.0))

@@ -4,21 +4,34 @@ from __future__ import annotations
 
 import numpy as np
 
-# Parity bar, per field f:  |cuda - oracle32| <= RTOL * max|oracle32_f|  (normwise, i.e. a
-# per-field absolute floor of RTOL * max|f|).  The float32 oracle itself sits at ~5e-6 of
-# max|f| from the float64 oracle on these fields: the tendencies are sums of terms that cancel,
-# so an elementwise 1e-5 bar would sit below float32's own rounding noise.  In addition the
-# CUDA path's error against the float64 oracle must not exceed X64_FACTOR times the float32
-# oracle's own error against float64, or within X64_FLOOR * max|f|.
+# Parity bar, per output field f, element by element:
+#
+#     |cuda - oracle32| <= RTOL * max(|oracle32|, ELEM_FLOOR[f] * max|oracle32_f|)
+#
+# i.e. relative error RTOL = 1e-5 above a per-field absolute floor.  Integer levels (iptop,
+# icltop) must match exactly.  Columns outside the bar must be trigger flips: a threshold test
+# of that column sits within FLIP_ULPS float32 ulps of its threshold in the oracle (counted, in
+# ulp buckets, and bounded).  The floors are the float32 conditioning of each field: the
+# temperature and humidity tendencies are sums of radiative, convective and diffusive terms
+# that cancel, and two float32 evaluations of the reference arithmetic that differ only in the
+# last bits of their exponentials already disagree by more than 1e-5 relative at elements below
+# these floors (tests/test_float32_sensitivity.py measures this on the oracle alone).  The
+# winds and precipitation take the floor 1e-3.  Normwise error <= RTOL * max|f| is asserted as
+# a second line, and the CUDA path's error against the float64 oracle must stay within
+# max(X64_FLOOR, X64_FACTOR x the float32 oracle's own).
 #
 # Diagnostic fields (cloud cover, surface radiation) carry more float32 noise than the
 # tendencies: cloud cover takes sqrt of a precipitation rate that is ~0 in most columns, so the
-# float32 oracle itself sits up to ~5e-5 of max|f| from float64 there.  Their bar is
+# float32 oracle itself sits up to ~5e-5 of max|f| from float64 there.  Their bar is normwise,
 # max(RTOL, NOISE_FACTOR * that float32-vs-float64 error), measured on the same inputs.  Their
 # float64 check runs the float64 oracle on the CUDA path's own precipitation
 # (conditional_diagnostics64), so that it tests the cloud and radiation arithmetic rather than
-# sqrt's magnification of precipitation rounding.
+# sqrt's magnification of precipitation rounding.  Their elementwise figures are reported.
 RTOL = 1e-5
+ELEM_FLOOR = {"u_wind": 1e-3, "v_wind": 1e-3, "precnv": 1e-3, "precls": 1e-3,
+              "temperature": 0.3, "specific_humidity": 0.1}
+REPORT_FLOOR = 1e-3  # the floor at which elementwise counts are also reported for every field
+FLIP_ULPS = 64
 NOISE_FACTOR = 2.0
 X64_FACTOR = 3.0
 X64_FLOOR = 1e-5
@@ -61,16 +74,23 @@ def column_mask(bad, shape2d):
     return b
 
 
-def oracle_f64(inst):
+def oracle_args(inst, params=None):
+    """The oracle's (state, forcing, geometry, date, params) for ``inst``; ``params`` is a dict
+    of parameter overrides keyed ``"group.name"`` (the oracle's naming)."""
+    from oracle import speedy_oracle as O
+    return inst.oracle_args(O.default_parameters(**(params or {})))
+
+
+def oracle_f64(inst, params=None):
     """The float64 oracle on the same (float32) input values: state, forcing and geometry
     fields are widened, vertical tables and parameters are rebuilt in float64."""
     from oracle import speedy_oracle as O
-    a32 = inst.oracle_args(O.default_parameters())
+    a32 = oracle_args(inst, params)
     st, fo, ge, da, _ = O.cast_inputs(*a32, np.float64)
     for n, v in zip(("hsg", "fsg", "dhs", "sigl", "grdsig", "grdscp", "wvi"),
                     O.vertical_tables(inst.kx, np.float64)):
         setattr(ge, n, v)
-    return st, fo, ge, da, O.default_parameters(np.float64)
+    return st, fo, ge, da, O.default_parameters(np.float64, **(params or {}))
 
 
 def normwise(a, b):
@@ -79,10 +99,34 @@ def normwise(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-30))
 
 
+def elementwise(g, r, floor):
+    """Elementwise relative error |g - r| / max(|r|, floor * max|r|)."""
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    scale = max(np.max(np.abs(r)), 1e-30)
+    return np.abs(g - r) / np.maximum(np.abs(r), floor * scale)
+
+
+def required_floor(g, r, keep=None, rtol=RTOL):
+    """The smallest floor (fraction of max|r|) at which every element (of the columns in
+    ``keep``) meets relative error rtol: max over elements with |g-r| > rtol |r| of
+    |g-r| / (rtol max|r|)."""
+    g = np.asarray(g, np.float64)
+    r = np.asarray(r, np.float64)
+    if keep is not None:
+        g, r = g[..., keep], r[..., keep]
+    if g.size == 0:
+        return 0.0
+    d = np.abs(g - r)
+    scale = max(np.max(np.abs(r)), 1e-30)
+    over = d > rtol * np.abs(r)
+    return float(np.max(d[over]) / (rtol * scale)) if over.any() else 0.0
+
+
 def compare_fields(got, tend, data, ref64=None, rtol=RTOL):
-    """Per-field report: normwise error, the tolerance applied and the elementwise failure
-    mask.  ``ref64`` (the float64 oracle's (tend, data)) sets the diagnostic fields' noise-aware
-    tolerance."""
+    """Per-field report: normwise error, the elementwise error above the field's floor, the
+    tolerance applied and the elementwise failure mask.  ``ref64`` (the float64 oracle's
+    (tend, data)) sets the diagnostic fields' noise-aware normwise tolerance."""
     ref = oracle_fields(tend, data)
     r64 = oracle_fields(*ref64) if ref64 is not None else None
     rep = {}
@@ -95,25 +139,37 @@ def compare_fields(got, tend, data, ref64=None, rtol=RTOL):
             bad = g != r
             rep[k] = dict(n=r.size, nbad=int(bad.sum()), norm=float(bad.mean()), tol=0.0, bad=bad)
             continue
-        tol = rtol
-        if k in DIAG_FIELDS and r64 is not None:
-            tol = max(rtol, NOISE_FACTOR * normwise(r, r64[k]))
         scale = max(np.max(np.abs(r)), 1e-30)
         err = np.abs(g - r)
-        bad = ~(err <= tol * scale)
-        rep[k] = dict(n=r.size, nbad=int(bad.sum()), norm=float(np.nanmax(err) / scale),
-                      tol=tol, bad=bad)
+        e_rep = elementwise(g, r, REPORT_FLOOR)
+        item = dict(n=r.size, norm=float(np.nanmax(err) / scale),
+                    elem_n_over_at_1e3=int((~(e_rep <= rtol)).sum()),
+                    elem_max_at_1e3=float(np.nanmax(e_rep)))
+        if k in DIAG_FIELDS:
+            tol = rtol
+            if r64 is not None:
+                tol = max(rtol, NOISE_FACTOR * normwise(r, r64[k]))
+            bad = ~(err <= tol * scale)
+            item.update(tol=tol, bad=bad, kind="normwise")
+        else:
+            floor = ELEM_FLOOR[k]
+            e = elementwise(g, r, floor)
+            bad = ~(e <= rtol)
+            item.update(tol=rtol, floor=floor, elem_max=float(np.nanmax(e)), bad=bad,
+                        bad_norm=~(err <= rtol * scale), kind="elementwise")
+        item["nbad"] = int(bad.sum())
+        rep[k] = item
     return rep
 
 
-def conditional_diagnostics64(inst, got, fuse_verify=False):
+def conditional_diagnostics64(inst, got, fuse_verify=False, params=None):
     """The float64 oracle with the CUDA path's precipitation substituted after the condensation
     term.  Cloud cover takes sqrt(precip) (shortwave_radiation.py:378), which magnifies the
     float32 rounding of a small precipitation rate without bound, and the surface radiation
     follows the cloud cover; evaluated on the precipitation the CUDA path produced (itself held
     to the 1e-5 bar), these diagnostics test the cloud and radiation arithmetic alone."""
     from oracle import speedy_oracle as O
-    st, fo, ge, da, p = oracle_f64(inst)
+    st, fo, ge, da, p = oracle_f64(inst, params)
     if fuse_verify:
         st = O.verify_state(st)
     kx, ix, il = st.temperature.shape
@@ -153,42 +209,95 @@ def x64_violations(errs):
 
 
 def parity_summary(rep, shape2d, margins_ulps=None):
-    """Columns failing tolerance, and how many of them sit near a threshold (trigger flips)."""
+    """Columns failing the bar, and how many of them sit near a threshold (trigger flips),
+    counted by the oracle's smallest threshold margin: within 1 ulp, within 4, within
+    FLIP_ULPS; the rest are unexplained."""
     cols = np.zeros(shape2d, bool)
     for v in rep.values():
         cols |= column_mask(v["bad"], shape2d)
     out = dict(bad_columns=int(cols.sum()), columns=int(np.prod(shape2d)))
     if margins_ulps is not None:
-        near = cols & (margins_ulps <= 64)
+        m = np.asarray(margins_ulps)
+        near = cols & (m <= FLIP_ULPS)
         out["flip_columns"] = int(near.sum())
-        out["unexplained_columns"] = int((cols & ~(margins_ulps <= 64)).sum())
-        out["max_margin_ulps_of_bad"] = float(np.max(margins_ulps[cols])) if cols.any() else 0.0
+        out["flip_columns_le_1ulp"] = int((cols & (m <= 1)).sum())
+        out["flip_columns_1_to_4ulp"] = int((cols & (m > 1) & (m <= 4)).sum())
+        out["flip_columns_4_to_64ulp"] = int((cols & (m > 4) & (m <= FLIP_ULPS)).sum())
+        out["unexplained_columns"] = int((cols & ~(m <= FLIP_ULPS)).sum())
+        out["max_margin_ulps_of_bad"] = float(np.max(m[cols])) if cols.any() else 0.0
     out["_cols"] = cols
     return out
+
+
+def oracle_step(kw):
+    from oracle import speedy_oracle as O
+    return O.physics_step if kw.get("fuse_verify") else O.compute_tendencies
+
+
+def oracle_kwargs(kw):
+    """The oracle-side keyword arguments of a SpeedyPhysics configuration."""
+    out = dict(orographic=bool(kw.get("orographic_correction")))
+    if kw.get("fuse_verify"):
+        if kw.get("time_step") is not None:
+            out["time_step"] = kw["time_step"]
+    return out
+
+
+def apply_q_scale(tend, scale):
+    """The humidity tendency unit scale the kernel fuses last (physics_interface.py:286)."""
+    if scale is not None and scale != 1.0:
+        dt = tend.specific_humidity.dtype.type
+        tend.specific_humidity = (tend.specific_humidity * dt(scale)).astype(
+            tend.specific_humidity.dtype)
+    return tend
+
+
+def check_against_oracle(inst, got, params=None, max_flip_frac=2e-3, label=None, **kw):
+    """Holds the CUDA results ``got`` of ``inst`` to the parity bar against the float32 and
+    float64 oracles; returns the per-field report and the column summary."""
+    from oracle import speedy_oracle as O
+    args = list(oracle_args(inst, params))
+    rec = O.Margins((inst.ix, inst.il))
+    step = oracle_step(kw)
+    okw = oracle_kwargs(kw)
+    tend, data = step(*args, rec=rec, **okw)
+    tend64, data64 = step(*oracle_f64(inst, params), **okw)
+    qs = kw.get("q_tend_scale")
+    tend, tend64 = apply_q_scale(tend, qs), apply_q_scale(tend64, qs)
+    rep = compare_fields(got, tend, data, (tend64, data64))
+    summ = parity_summary(rep, (inst.ix, inst.il), rec.ulps)
+    cols = summ.pop("_cols")
+    cond = conditional_diagnostics64(inst, got, fuse_verify=bool(kw.get("fuse_verify")),
+                                     params=params)
+    x64 = x64_errors(got, tend, data, (tend64, data64), exclude_cols=cols, cond64=cond)
+    keep = ~cols
+    norm_bad = {k: int(column_mask(v["bad_norm"], cols.shape)[keep].sum())
+                for k, v in rep.items() if "bad_norm" in v}
+    floors = {k: round(required_floor(got[k], oracle_fields(tend, data)[k], keep), 4)
+              for k in STRICT_FIELDS if k in got}
+    print(label or inst.name,
+          {k: (v["nbad"], f"{v['norm']:.1e}", f"e{v.get('elem_max', 0):.1e}",
+               v["elem_n_over_at_1e3"]) for k, v in rep.items() if k in FLOAT_FIELDS},
+          {k: v for k, v in summ.items()},
+          "required floors", floors,
+          {k: (f"{a:.1e}", f"{b:.1e}") for k, (a, b) in x64.items()})
+    assert summ["unexplained_columns"] == 0, (summ, {k: v["nbad"] for k, v in rep.items()})
+    assert summ["flip_columns"] <= max(2, max_flip_frac * summ["columns"]), summ
+    assert not any(norm_bad.values()), norm_bad
+    assert not x64_violations(x64), x64_violations(x64)
+    summ["required_floors"] = floors
+    return rep, summ
 
 
 def parity_check(pkg, inst, params=None, max_flip_frac=2e-3, device="cuda", **kw):
     """Run ``inst`` through the CUDA path and hold it to the parity bar against the float32
     and float64 oracles; returns the per-field report and the column summary."""
-    from oracle import speedy_oracle as O
-    got = run_gpu_instance(pkg, inst, device=device, params=params, **kw)
-    args = list(inst.oracle_args(O.default_parameters()))
-    rec = O.Margins((inst.ix, inst.il))
-    step = O.physics_step if kw.get("fuse_verify") else O.compute_tendencies
-    oro = bool(kw.get("orographic_correction"))
-    tend, data = step(*args, rec=rec, orographic=oro)
-    ref64 = step(*oracle_f64(inst), orographic=oro)
-    rep = compare_fields(got, tend, data, ref64)
-    summ = parity_summary(rep, (inst.ix, inst.il), rec.ulps)
-    cols = summ.pop("_cols")
-    cond = conditional_diagnostics64(inst, got, fuse_verify=bool(kw.get("fuse_verify")))
-    x64 = x64_errors(got, tend, data, ref64, exclude_cols=cols, cond64=cond)
-    print(inst.name, {k: (v["nbad"], f"{v['norm']:.1e}") for k, v in rep.items()}, summ,
-          {k: (f"{a:.1e}", f"{b:.1e}") for k, (a, b) in x64.items()})
-    assert summ["unexplained_columns"] == 0, (summ, {k: v["nbad"] for k, v in rep.items()})
-    assert summ["flip_columns"] <= max(2, max_flip_frac * summ["columns"]), summ
-    assert not x64_violations(x64), x64_violations(x64)
-    return rep, summ
+    phys_params = None
+    if params:
+        phys_params = pkg.Parameters.default().with_values(
+            **{k.replace(".", "__"): v for k, v in params.items()})
+    got = run_gpu_instance(pkg, inst, device=device, params=phys_params, **kw)
+    return check_against_oracle(inst, got, params=params, max_flip_frac=max_flip_frac, **kw)
 
 
 def fake_fields(L, base=1 << 36, spacing=1 << 28):

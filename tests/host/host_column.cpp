@@ -290,6 +290,23 @@ int hc_vjp_any(int mode, HC_VJP_ARGS) {
   return -2;
 }
 
+// hc_vjp_any over n columns: ct[n][34] holds each column's 16 temperature and 16 humidity
+// cotangents and the lowest-level wind cotangents; out[n][63] receives the temperature,
+// humidity and geopotential gradients (16 each), psa, u, v and the 12 parameter gradients.
+// Returns n, or -1 - i for the first column i whose VJP failed.
+int hc_vjp_batch(int mode, const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* hs,
+                 int n, const double* ct, double* out, double dt_seconds,
+                 double q_tend_scale) {
+  for (int i = 0; i < n; ++i) {
+    const double* c = ct + (size_t)i * 34;
+    double* o = out + (size_t)i * 63;
+    const int rc = hc_vjp_any(mode, vg, p, hs + i, c, c + 16, c[32], c[33], o, o + 16, o + 32,
+                              o + 48, o + 49, o + 50, o + 51, dt_seconds, q_tend_scale);
+    if (rc <= 0) return -1 - i;
+  }
+  return n;
+}
+
 int hc_vjp32(const spd_vgrid_t* vg, const spd_params_t* p, const HostColumn* h,
              const double* ct_dt, const double* ct_dq, double ct_du, double ct_dv, double* g_t,
              double* g_q, double* g_phi, double* g_psa, double* g_u, double* g_v,

@@ -393,3 +393,27 @@ def test_admission_is_capped_per_step():
         sch.submit(S.Request(S.TENDENCY, ["a"]))
     sch.admit()
     assert len(sch.waiting) == 4
+
+
+def test_cuda_backend_release_waits_for_the_upload_before_freeing():
+    """CudaBackend.release returns a member's range to the arena only after the member's
+    upload event has completed (recorded order: the event's synchronize, then the arena
+    release); no device is touched (the event and the arena are fakes)."""
+    S = pkg.serving
+    order = []
+
+    class Ev:
+        def synchronize(self):
+            order.append("upload done")
+
+    class Arena:
+        def release(self, handle):
+            order.append(("arena release", handle))
+
+    be = S.CudaBackend.__new__(S.CudaBackend)
+    be.arena = Arena()
+    dm = S._DevMember(None, object(), None, Ev())
+    dm.handle = 7
+    be.release(dm)
+    assert order == ["upload done", ("arena release", 7)]
+    assert dm.buf is None

@@ -4,9 +4,10 @@ A foreign-function bridge that only forwards the buffers it was handed, or a pro
 device memory is owned by another runtime's allocator, cannot provide spd_fwd's scratch
 buffer.  spd_fwd_noalloc keeps that scratch in a fixed array inside the library instead.  The
 GPU test calls it through the C ABI twice in a row, on two different instances (so the
-second call runs over the first call's leftovers in the shared array), and checks both
-results against spd_fwd's under the parity tolerance.  This file is collected last on
-purpose.
+second call runs over the first call's leftovers in the shared array), and checks that both
+results equal spd_fwd's bitwise: both entry points run the same two kernels over the same
+one-member plan, so any difference would be a scratch offset or leftover-state fault.  This
+file is collected last on purpose.
 """
 import ctypes as C
 import importlib
@@ -14,7 +15,7 @@ import importlib
 import numpy as np
 import pytest
 
-from tests.helpers import RTOL, fake_fields, to_device
+from tests.helpers import fake_fields, to_device
 
 
 @pytest.fixture(scope="module")
@@ -71,11 +72,9 @@ def test_noalloc_matches_spd_fwd_on_two_calls_in_a_row(pkg):
         assert rc == 0, lib.spd_status_string(rc)
         torch.cuda.synchronize()
         for k, r in ref.items():
-            g = out[k].cpu().numpy().astype(np.float64)
-            r = r.cpu().numpy().astype(np.float64)
+            g = out[k].cpu().numpy()
             assert np.all(np.isfinite(g)), k
-            scale = max(np.max(np.abs(r)), 1e-30)
-            assert np.max(np.abs(g - r)) <= RTOL * scale, k
+            assert np.array_equal(g, r.cpu().numpy()), k
 
 
 def test_noalloc_rejects_too_many_latitudes(pkg):
