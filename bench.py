@@ -28,18 +28,11 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM bytes (read + write) per column of the dominant kernel's launch (the second launch,
-# ensemble_columns), from one ncu capture each (profiles/ensemble_columns_ragged_ensemble.md:
-# 179.1 MB read + 48.4 MB written over 466,944 columns; profiles/ensemble_columns_t425.md:
-# 370.4 + 156.4 MB over 819,200 columns).  Part of each launch's writes is still in L2 when the
-# kernel ends, so the write share reads low.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": (179.083264e6 + 48.404224e6) / 466944,
-                          "t425": (370.373120e6 + 156.422400e6) / 819200}
-# Warp instructions per launch of the dominant kernel (smsp__inst_executed.sum, same captures):
-# the compute side of the roofline, against one instruction per scheduler per cycle.  The
-# adjoint's is ensemble_adjoint at T170 with 16 levels (profiles/ensemble_adjoint_t170.md).
-NCU_WARP_INSTRUCTIONS = {"ensemble": 80446120.0, "t425": 170901355.0,
-                         "adjoint_t170": 117031373.0}
+# DRAM bytes (read + write) per column of the dominant kernel (ensemble_fused) and its warp
+# instructions per launch, from one ncu capture each (the commands and figures are in the
+# profiles/ summaries named for the kernel and workload); None until captured.
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": None, "t425": None}
+NCU_WARP_INSTRUCTIONS = {"ensemble": None, "t425": None, "adjoint_t170": 117031373.0}
 
 
 def parse_args():
@@ -170,9 +163,9 @@ def run_b200(args):
 
     members = workload_members(pkg, args.workload, rank)
     cols = sum(m.columns for m in members)
-    bytes_step = sum(pkg.synthetic.fwd_bytes(m.kx, m.columns) for m in members)
-    bytes_first = sum(pkg.synthetic.first_half_bytes(m.kx, m.columns) for m in members)
-    bytes_second = sum(pkg.synthetic.second_half_bytes(m.kx, m.columns) for m in members)
+    bytes_path = sum(pkg.synthetic.path_bytes(m.kx, m.columns) for m in members)
+    bytes_min = sum(pkg.synthetic.fwd_bytes(m.kx, m.columns) for m in members)
+    bytes_lvl = sum(pkg.synthetic.levelset_bytes(m.kx, m.columns) for m in members)
 
     # device-resident inputs and preallocated outputs
     runs = []
@@ -225,15 +218,14 @@ def run_b200(args):
         return max_over_ranks(e0.elapsed_time(e1), dist, dev)
 
     # The timed region: K steps between two events.  A second pass records a marker event
-    # between the two launches of every step (batched mode) so that each launch is timed alone.
+    # between the two launches of every step (batched mode) so that each launch is timed alone;
+    # a third runs steps back to back for at least a second while nvidia-smi samples the clocks
+    # (the K-step region is a few milliseconds, shorter than one clock sample).
     marks = [(primed_event(), primed_event(), primed_event()) for _ in range(args.steps)]
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     barrier()
-    clocks = ClockSampler(dev.index)
-    clocks.start()
-    time.sleep(0.3)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -242,7 +234,24 @@ def run_b200(args):
     e1.record()
     torch.cuda.synchronize()
     barrier()
+    total_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    ms_step = total_ms / args.steps
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    time.sleep(0.3)
+    reps_1s = max(args.steps, int(1000.0 / max(ms_step, 1e-3)) + 1)
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    c0.record()
+    for _ in range(reps_1s):
+        step()
+    c1.record()
+    torch.cuda.synchronize()
     clk = clocks.stop()
+    ms_step_1s = c0.elapsed_time(c1) / reps_1s
+    if clk is not None:
+        clk["window"] = f"{reps_1s} steps back to back, {c0.elapsed_time(c1):.0f} ms"
+    barrier()
     # the two launches timed apart, in a separate pass of as many steps (a marker event between
     # them serialises them in plain stream order; the timed steps above overlap them)
     if ens is not None:
@@ -251,8 +260,6 @@ def run_b200(args):
             step(marker=m)
             b.record()
         torch.cuda.synchronize()
-    total_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
-    ms_step = total_ms / args.steps
     col_ms = pre_ms = None
     if ens is not None:
         col_ms = sum(m.elapsed_time(b) for (a, m, b) in marks) / args.steps
@@ -266,31 +273,38 @@ def run_b200(args):
                  "launches_per_step": 2 * len(runs),
                  "batched_over_plain": round(pms / ms_step, 2)}
 
-    # roofline of the dominant kernel (the second launch, radiation through vertical diffusion):
-    # the bytes that launch must move (its inputs and the first launch's stage read once, its
-    # outputs written once) over its own event-timed duration; the first launch and the whole
-    # step (the path's own inputs and outputs, once) beside it
+    # Roofline of the dominant kernel, ensemble_fused (every column whole): the path's
+    # algorithmic bytes, 4 (9 kx + 12) per column (u and v at every level read, the four
+    # tendency planes and the precipitation written, once each), over its own event-timed
+    # duration.  Beside it: the same over the whole step (both launches), the bytes the kernel
+    # must move at least (4 (7 kx + 14): the physics reads u and v at the lowest level only),
+    # and the level-set launch, whose reads of T, q, phi and psa repeat the fused launch's.
     peak, peak_kind = load_peaks()
     kern_ms = col_ms if col_ms is not None else ms_step
     two = col_ms is not None
-    achieved = (bytes_second if two else bytes_step) / (kern_ms / 1e3) / 1e9
+    achieved = bytes_path / (kern_ms / 1e3) / 1e9
     traffic = NCU_TRAFFIC_PER_COLUMN.get(args.workload)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "kernel": ("ensemble_columns" if two
-                           else "ensemble_moist + ensemble_columns (one forward per member)"),
+                "kernel": ("ensemble_fused" if two
+                           else "ensemble_levelset + ensemble_fused (one forward per member)"),
                 "kernel_ms": round(kern_ms, 4),
-                "algorithmic_bytes_per_launch": bytes_second if two else bytes_step,
-                "traffic": (round(traffic * cols) if traffic else None)}
+                "algorithmic_bytes_per_launch": bytes_path,
+                "bytes_per_column": "4 (9 kx + 12)",
+                "traffic": (round(traffic * cols) if traffic else None),
+                "traffic_over_algorithmic": (round(traffic * cols / bytes_path, 3)
+                                             if traffic else None),
+                "kernel_minimum_bytes": bytes_min,
+                "kernel_minimum_frac": round(bytes_min / (kern_ms / 1e3) / 1e9 / peak, 4),
+                "step": {"ms": round(ms_step, 4),
+                         "achieved_gbs": round(bytes_path / (ms_step / 1e3) / 1e9, 1),
+                         "frac": round(bytes_path / (ms_step / 1e3) / 1e9 / peak, 4)}}
     if two:
-        roofline["first_launch"] = {
-            "kernel": "ensemble_moist", "ms": round(pre_ms, 4),
-            "algorithmic_bytes": bytes_first,
-            "achieved_gbs": round(bytes_first / (pre_ms / 1e3) / 1e9, 1)}
-        roofline["step"] = {"path_algorithmic_bytes": bytes_step, "ms": round(ms_step, 4),
-                            "achieved_gbs": round(bytes_step / (ms_step / 1e3) / 1e9, 1)}
-    # the bound that governs this kernel: instruction issue (one warp instruction per scheduler
-    # per cycle), with the instruction count of the ncu capture and the SM clock sampled here
+        roofline["levelset_launch"] = {
+            "kernel": "ensemble_levelset", "ms": round(pre_ms, 4), "bytes_read": bytes_lvl,
+            "achieved_gbs": round(bytes_lvl / (pre_ms / 1e3) / 1e9, 1)}
+    # the issue bound: one warp instruction per scheduler per cycle, with the instruction count
+    # of the ncu capture and the SM clock sampled here
     insts = NCU_WARP_INSTRUCTIONS.get(args.workload)
     issue = None
     if insts and clk and world == 1:
@@ -397,14 +411,16 @@ def run_b200(args):
     if rank == 0:
         line = {"metric": "physics columns/s", "value": round(value, 1), "unit": "columns/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+                "ms_per_step": round(ms_step, 4), "ms_per_step_1s_loop": round(ms_step_1s, 4),
+                "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded generators with the workload's shapes and distributions)",
                 "config": workload_config(args.workload, members, args.mode),
                 "roofline": roofline, "issue_roofline": issue, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk,
                 "plain": plain, "grid_blocks": grid_blocks,
-                "gpu_launches": launches_per_step * args.steps}
+                "gpu_launches": launches_per_step * args.steps,
+                "gpu_launches_note": "launches of this library's kernels in the K timed steps"}
         line.update(sections)
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -493,30 +509,34 @@ def t425_section(pkg, dev, peak, peak_kind, sm_mhz=None):
             call()
     graph_ms = event_ms(g.replay, 5, warmup=3) / 24
     cols = inst.columns
-    nbytes = pkg.synthetic.fwd_bytes(inst.kx, cols)
-    b2 = pkg.synthetic.second_half_bytes(inst.kx, cols)
-    b1 = pkg.synthetic.first_half_bytes(inst.kx, cols)
-    bw = b2 / (col_ms / 1e3) / 1e9
+    nbytes = pkg.synthetic.path_bytes(inst.kx, cols)
+    nmin = pkg.synthetic.fwd_bytes(inst.kx, cols)
+    blvl = pkg.synthetic.levelset_bytes(inst.kx, cols)
+    bw = nbytes / (col_ms / 1e3) / 1e9
     out_d = {"workload": "T425 1280x640, 16 levels, one instance", "columns": cols,
              "path_algorithmic_bytes_per_call": nbytes,
              "plain_call_ms": round(call_ms, 4),
              "plain_call_launches_apart_ms": round(marked_ms, 4),
-             "first_launch_ms": round(first_ms, 4),
-             "second_launch_ms": round(col_ms, 4),
+             "levelset_launch_ms": round(first_ms, 4),
+             "fused_launch_ms": round(col_ms, 4),
              "graph_24_calls_ms_per_call": round(graph_ms, 4),
              "columns_per_s_plain": round(cols / (call_ms / 1e3), 1),
              "columns_per_s_graph": round(cols / (graph_ms / 1e3), 1),
-             "first_launch_algorithmic_bytes": b1,
-             "first_launch_hbm_gbs": round(b1 / (first_ms / 1e3) / 1e9, 1),
-             "second_launch_algorithmic_bytes": b2,
-             "second_launch_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
-             "second_launch_hbm_frac": round(bw / peak, 4),
-             "second_launch_traffic": round(NCU_TRAFFIC_PER_COLUMN["t425"] * cols)}
-    if sm_mhz:
+             "levelset_launch_bytes_read": blvl,
+             "levelset_launch_hbm_gbs": round(blvl / (first_ms / 1e3) / 1e9, 1),
+             "fused_launch_hbm_gbs": round(bw, 1), "peak_gbs": peak, "peak_kind": peak_kind,
+             "fused_launch_hbm_frac": round(bw / peak, 4),
+             "fused_launch_kernel_minimum_frac": round(nmin / (col_ms / 1e3) / 1e9 / peak, 4),
+             "plain_call_hbm_frac": round(nbytes / (call_ms / 1e3) / 1e9 / peak, 4),
+             "graph_call_hbm_frac": round(nbytes / (graph_ms / 1e3) / 1e9 / peak, 4)}
+    t = NCU_TRAFFIC_PER_COLUMN.get("t425")
+    if t:
+        out_d["fused_launch_traffic"] = round(t * cols)
+    if sm_mhz and NCU_WARP_INSTRUCTIONS.get("t425"):
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         peak_issue = sms * 4 * sm_mhz * 1e6
         ach = NCU_WARP_INSTRUCTIONS["t425"] / (col_ms / 1e3)
-        out_d["second_launch_issue_frac"] = round(ach / peak_issue, 4)
+        out_d["fused_launch_issue_frac"] = round(ach / peak_issue, 4)
         out_d["issue_roofline_note"] = ("warp instructions per launch from ncu over one "
                                         "instruction per scheduler per cycle at the sampled "
                                         "SM clock")
@@ -621,66 +641,63 @@ def serving_section(pkg, dev, n_requests):
     return out
 
 
-_MEMBER_CACHE = {}
-
-
-def _oracle_member(args):
-    """Runs the oracle on one member in a worker process (inputs generated once per worker)."""
-    import importlib as il
+def cpu_baseline(members, min_seconds=10.0):
+    """The compiled CPU restatement of the reference physics (oracle/cpu_port.cpp: float32,
+    -O3 without fast-math, OpenMP) over the whole workload on every host core, repeated for at
+    least ``min_seconds``; columns/s.  The NumPy port (the oracle) on one core beside it as a
+    cross-check."""
+    from oracle import cpu_port
     from oracle import speedy_oracle as O
-    if args not in _MEMBER_CACHE:
-        pkg = il.import_module("jax-gcm_b200")
-        kind, seed, ix, il_, kx = args
-        inst = pkg.synthetic.land_instance(seed, ix, il_, kx)
-        _MEMBER_CACHE[args] = (inst.columns, inst.oracle_args(O.default_parameters()))
-    cols, oargs = _MEMBER_CACHE[args]
-    t0 = time.perf_counter()
-    O.compute_tendencies(*oargs)
-    return cols, time.perf_counter() - t0
-
-
-def cpu_baseline(members, repeats=2):
-    """The oracle (NumPy port of the reference physics) on one host core over the whole
-    workload, repeated; columns/s."""
-    from oracle import speedy_oracle as O
-    done, secs = 0, 0.0
-    for _ in range(repeats):
-        for m in members:
-            args = m.oracle_args(O.default_parameters())
-            t0 = time.perf_counter()
-            O.compute_tendencies(*args)
-            secs += time.perf_counter() - t0
-            done += m.columns
-    return {"value": round(done / secs, 1), "unit": "columns/s", "cores": 1, "kind": "port",
-            "sample": f"{repeats} passes of the NumPy oracle over all {len(members)} members "
-                      f"({sum(m.columns for m in members)} columns), one core"}
+    cores = os.cpu_count() or 1
+    batch = cpu_port.Batch(members)
+    batch.run(nthreads=cores)
+    passes, t0 = 0, time.perf_counter()
+    while True:
+        batch.run(nthreads=cores)
+        passes += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds:
+            break
+    value = passes * batch.columns / el
+    # NumPy cross-check: one pass over a sample of members, one core
+    sample = members[:: max(1, len(members) // 8)]
+    np_cols, np_secs = 0, 0.0
+    for m in sample:
+        args = m.oracle_args(O.default_parameters())
+        t1 = time.perf_counter()
+        O.compute_tendencies(*args)
+        np_secs += time.perf_counter() - t1
+        np_cols += m.columns
+    return {"value": round(value, 1), "unit": "columns/s", "cores": cores, "kind": "port",
+            "sample": f"{passes} passes of the compiled C++ port of the reference physics "
+                      f"(oracle/cpu_port.cpp, float32, -O3, no fast-math, OpenMP) over all "
+                      f"{len(members)} members ({batch.columns} columns) on {cores} threads, "
+                      f"{el:.1f} s",
+            "numpy_port_one_core": {"value": round(np_cols / np_secs, 1),
+                                    "sample": f"the NumPy oracle over {len(sample)} of the "
+                                              f"members ({np_cols} columns), one core"}}
 
 
 def run_reference(args):
-    """The reference arm: the CPU port of the reference physics on all host cores."""
+    """The reference arm: the compiled CPU port of the reference physics on all host cores,
+    one step = one pass over the workload's members."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import multiprocessing as mp
+    from oracle import cpu_port
     pkg = importlib.import_module("jax-gcm_b200")
     members = workload_members(pkg, args.workload, 0)
-    jobs = []
-    for n, m in enumerate(members):
-        jobs.append(("land", 1000 + n, m.ix, m.il, m.kx))
     cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    cols = sum(m.columns for m in members)
-    with ctx.Pool(cores) as pool:
-        for _ in range(max(1, args.warmup)):
-            pool.map(_oracle_member, jobs, chunksize=1)
-        t0 = time.perf_counter()
-        done = 0
-        for _ in range(args.steps):
-            res = pool.map(_oracle_member, jobs, chunksize=1)
-            done += sum(r[0] for r in res)
-        el = time.perf_counter() - t0
-    value = done / el
+    batch = cpu_port.Batch(members)
+    for _ in range(max(1, args.warmup)):
+        batch.run(nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.run(nthreads=cores)
+    el = time.perf_counter() - t0
+    value = args.steps * batch.columns / el
+    cols = batch.columns
     line = {"impl": "reference", "metric": "physics columns/s", "value": round(value, 1),
             "unit": "columns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True,
@@ -689,9 +706,10 @@ def run_reference(args):
             "config": workload_config(args.workload, members, "reference"),
             "cpu_baseline": {"value": round(value, 1), "unit": "columns/s", "cores": cores,
                              "kind": "port",
-                             "sample": f"each step: the NumPy port of the reference physics over "
-                                       f"all {len(members)} members ({cols} columns) spread "
-                                       f"over {cores} worker processes (inputs pre-generated)"},
+                             "sample": f"each step: the compiled C++ port of the reference "
+                                       f"physics (oracle/cpu_port.cpp, float32, -O3, no "
+                                       f"fast-math, OpenMP) over all {len(members)} members "
+                                       f"({cols} columns) on {cores} threads"},
             "e2e": {"value": round(value, 1), "unit": "columns/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -18,8 +18,8 @@
  *    synchronisation and allocates no memory; scratch is caller-provided.
  *  - Return value 0 (SPD_OK) or one of the SPD_ERR_* codes; no exceptions cross the ABI.
  *  - The forward's output fields overlap neither its input fields nor one another
- *    (SPD_ERR_ALIAS): between its two launches the forward keeps intermediate per-column
- *    values in its own output planes.
+ *    (SPD_ERR_ALIAS): columns write their outputs while other columns still read their
+ *    inputs, and its level-set launch reads the state before any output is written.
  */
 #ifndef SPEEDY_B200_H
 #define SPEEDY_B200_H
@@ -61,12 +61,18 @@ enum spd_flags {
                                  speedy_physics.py:65,79).  Its tendency divides by
                                  spd_desc_t.dt_seconds, which must then equal
                                  DateData.dt_seconds. */
-  SPD_ACCUMULATE_DIAGNOSTICS = 1u << 6
+  SPD_ACCUMULATE_DIAGNOSTICS = 1u << 6,
   /* The forward adds precnv, precls and every non-NULL float diagnostic to what the output
    * buffers hold (out[c] += value) instead of overwriting them; the tendency planes and the
    * integer levels are written as usual.  This is DiagnosticsCollector's running average
    * (jcm/model.py:46-64: data[i] += new / steps) without a pass over PhysicsData per physics
    * step: zero the buffers, make the steps' calls, scale by 1/steps once. */
+  SPD_LOW_LEVEL_WINDS = 1u << 7
+  /* Forward only: spd_inputs_t.u_wind / v_wind and spd_outputs_t.u_wind / v_wind are single
+   * [ix][il] planes holding the lowest level.  The physics reads the winds at the lowest level
+   * only (surface_flux.py:57-58) and its wind tendencies are zero above it (surface_flux.py
+   * :294-295), so a caller that keeps those zeros itself moves 2 (kx - 1) fewer planes each
+   * way (the reference returns dense [kx][ix][il] planes; the default writes them). */
 };
 
 /* One grid instance: shape, switches and DateData (jcm/date.py:9-14). */
@@ -140,13 +146,13 @@ typedef struct {
 size_t spd_fwd_scratch_bytes(const spd_desc_t* desc);
 
 /* SpeedyPhysics.compute_tendencies for one instance (speedy_physics.py:88-127).
- * Two launches on `stream`, each over every column: the first half of the column physics
- * (humidity, convection, large-scale condensation, clouds), which also forms the instance's
- * cloud-top level set (shortwave_radiation.py:62-68) and leaves intermediate values in the
- * output planes; then the second half (radiation, surface fluxes, vertical diffusion), which
- * writes every output.  They are the batched kernels below run on a one-member plan, so the
- * results equal the batched path's bitwise.  `scratch` must be 256-byte aligned and at least
- * spd_fwd_scratch_bytes(desc) long; it is initialised by the call. */
+ * Two launches on `stream`, each over every column: a light one that forms the instance's
+ * cloud-top level set (shortwave_radiation.py:62-68: the cloud tops of every column, from
+ * humidity, convection, condensation and clouds) and its per-latitude solar table; then every
+ * column whole in one pass (all terms, verify_tendencies when on, every output).  They are the
+ * batched kernels below run on a one-member plan, so the results equal the batched path's
+ * bitwise.  `scratch` must be 256-byte aligned and at least spd_fwd_scratch_bytes(desc) long;
+ * it is initialised by the call. */
 int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
             const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
             size_t scratch_bytes, void* stream);
@@ -154,8 +160,9 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 /* Timing hook (no reference counterpart): spd_fwd, recording `event` (a cudaEvent_t, or NULL)
  * on `stream` between its two launches, so that a caller can time them separately with
  * events.  With an event the launches run in plain stream order; without one (and in spd_fwd)
- * the second launch is a programmatic dependent launch that starts as the first one's blocks
- * retire and waits on the device for its completion before reading its results. */
+ * the second launch is a programmatic dependent launch: its blocks start as the first one's
+ * retire and run the first half of their columns, then wait on the device for the first
+ * launch's completion before reading the level set and the solar table. */
 int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
                    const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
                    size_t scratch_bytes, void* stream, void* event);
@@ -283,7 +290,7 @@ int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 
 /* Timing hook (no reference counterpart): spd_ensemble_fwd, recording `event` (a cudaEvent_t,
- * or NULL) on `stream` between its two launches (the first and the second half), which then
+ * or NULL) on `stream` between its two launches (the level sets and the columns), which then
  * run in plain stream order (see spd_fwd_marked). */
 int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
                             const spd_plan_info_t* info, int grid_blocks, void* stream,

@@ -21,6 +21,7 @@ SPD_INCREASE_CO2 = 1 << 3
 SPD_FUSE_VERIFY = 1 << 4
 SPD_OROGRAPHIC = 1 << 5
 SPD_ACCUMULATE_DIAGNOSTICS = 1 << 6
+SPD_LOW_LEVEL_WINDS = 1 << 7
 
 
 class Desc(C.Structure):

@@ -37,8 +37,9 @@ class Ensemble:
 
     def __init__(self, members: List[Member], date, parameters: Optional[Parameters] = None,
                  fuse_verify=False, time_step=None, q_tend_scale=1.0,
-                 orographic_correction=False):
+                 orographic_correction=False, low_level_winds=False):
         lib = _lib.load()
+        self.low_level_winds = low_level_winds
         self.members = members
         self.date = date
         self.phys = SpeedyPhysics(parameters, fuse_verify=fuse_verify, time_step=time_step,
@@ -61,6 +62,8 @@ class Ensemble:
                 keys[key] = len(classes)
                 c = _lib.Class()
                 c.desc = self.phys.desc(g, date, m.forcing.lfluxland)
+                if low_level_winds:  # u, v and their tendencies as lowest-level planes
+                    c.desc.flags |= _lib.SPD_LOW_LEVEL_WINDS
                 c.vgrid = g.vgrid()
                 c.params = self.phys._pstruct
                 classes.append(c)
@@ -83,10 +86,15 @@ class Ensemble:
             for k, v in tensors.items():
                 if v.dtype != torch.float32 or not v.is_contiguous() or v.device != dev:
                     raise ValueError(f"member {i}: field {k} must be contiguous float32 on {dev}")
+            wind_numel = ix * il if low_level_winds else kx * ix * il
+            for k in ("u_wind", "v_wind"):
+                if tensors[k].numel() != wind_numel:
+                    raise ValueError(f"member {i}: {k} must have {wind_numel} elements")
             if m.out is None:
                 e3 = lambda: torch.empty((kx, ix, il), dtype=torch.float32, device=dev)
                 e2 = lambda: torch.empty((ix, il), dtype=torch.float32, device=dev)
-                m.out = dict(u_wind=e3(), v_wind=e3(), temperature=e3(), specific_humidity=e3(),
+                ew = e2 if low_level_winds else e3
+                m.out = dict(u_wind=ew(), v_wind=ew(), temperature=e3(), specific_humidity=e3(),
                              precnv=e2(), precls=e2())
             mem[i].inp = _lib.Inputs(**{k: tensors[k].data_ptr() for k in _lib.INPUT_FIELDS})
             mem[i].out = _lib.Outputs(**{k: (m.out[k].data_ptr() if k in m.out else None)
@@ -189,22 +197,28 @@ def _packed_layout(members, fields, level_fields):
 class HostPipeline:
     """Ensemble steps whose state comes from, and whose results go to, pinned host memory.
 
-    Every member's state (u, v, T, q, phi, psa) lives in one packed host buffer and every
-    member's results (the four tendency planes, precnv, precls) in another, so a step is one
-    host-to-device copy, one ``spd_ensemble_fwd`` and one device-to-host copy.  ``depth`` sets of
-    device buffers (each with its own plan) rotate over three streams: while step n computes,
-    step n+1's state uploads and step n-1's results download (PCIe carries both directions at
-    once).  Forcing and geometry stay resident.
+    Every member's state (T, q and phi at every level, u and v at the lowest level, psa) lives
+    in one packed host buffer and every member's results (the T and q tendency planes, the
+    lowest-level u and v tendencies, precnv, precls) in another, so a step is one host-to-device
+    copy, one ``spd_ensemble_fwd`` and one device-to-host copy.  Only the lowest wind level
+    crosses PCIe in either direction: the physics reads the winds there alone
+    (surface_flux.py:57-58) and its wind tendencies are zero above it (surface_flux.py:294-295),
+    so the ensemble runs with SPD_LOW_LEVEL_WINDS.  ``depth`` sets of device buffers (each with
+    its own plan) rotate over three streams: while step n computes, step n+1's state uploads and
+    step n-1's results download (PCIe carries both directions at once).  Forcing and geometry
+    stay resident.
 
     ``host_state`` (pack into it with ``set_state``) is read by every step; ``submit()`` enqueues
     one step and returns the index of the host result buffer it writes; ``wait(i)`` blocks until
-    that buffer is complete and ``results(i)`` views it per member.
+    that buffer is complete and ``results(i)`` views it per member (u and v tendencies as the
+    lowest-level [ix, il] plane; ``dense_winds`` gives the reference's [kx, ix, il] form).
     """
 
     def __init__(self, members: List[Member], date, depth: int = 2, **ensemble_kw):
         dev = members[0].state.temperature.device
         self.device, self.depth = dev, depth
-        level = {"u_wind", "v_wind", "temperature", "specific_humidity", "geopotential"}
+        level = {"temperature", "specific_humidity", "geopotential"}
+        self.kx = [m.geometry.nodal_shape[0] for m in members]
         self.in_layout, n_in = _packed_layout(members, STATE_FIELDS, level)
         self.out_layout, n_out = _packed_layout(members, RESULT_FIELDS, level)
         self.host_state = torch.empty(n_in, dtype=torch.float32, pin_memory=True)
@@ -222,7 +236,7 @@ class HostPipeline:
                 ov = {f: self._view(self.dev_results[b], *lo[f]) for f in RESULT_FIELDS}
                 st = type(m.state)(*(sv[f] for f in STATE_FIELDS))
                 mem.append(Member(st, m.forcing, m.geometry, ov))
-            self.ensembles.append(Ensemble(mem, date, **ensemble_kw))
+            self.ensembles.append(Ensemble(mem, date, low_level_winds=True, **ensemble_kw))
         self.h2d = torch.cuda.Stream(dev)
         self.compute = torch.cuda.Stream(dev)
         self.d2h = torch.cuda.Stream(dev)
@@ -239,9 +253,13 @@ class HostPipeline:
         return flat[off:off + n].view(shape)
 
     def set_state(self, i, state):
-        """Packs member i's state (a PhysicsState of CPU or CUDA tensors) into host_state."""
+        """Packs member i's state (a PhysicsState of CPU or CUDA tensors, winds at every level)
+        into host_state; of u and v only the lowest level is kept."""
         for f in STATE_FIELDS:
-            self._view(self.host_state, *self.in_layout[i][f]).copy_(getattr(state, f))
+            x = getattr(state, f)
+            if f in ("u_wind", "v_wind"):
+                x = x[-1]
+            self._view(self.host_state, *self.in_layout[i][f]).copy_(x)
 
     def begin(self):
         """Orders the pipeline's streams after the work already on the current stream."""
@@ -283,6 +301,13 @@ class HostPipeline:
         """Member views of host result buffer i: [{field: tensor}] (valid after wait(i))."""
         return [{f: self._view(self.host_results[i], *lo[f]) for f in RESULT_FIELDS}
                 for lo in self.out_layout]
+
+    def dense_winds(self, i, plane):
+        """The reference's dense [kx, ix, il] wind tendency of member i from its lowest-level
+        plane (zeros above)."""
+        out = torch.zeros((self.kx[i],) + tuple(plane.shape), dtype=plane.dtype)
+        out[-1] = plane
+        return out
 
     @property
     def h2d_bytes(self):

@@ -22,13 +22,18 @@ OUT = os.path.join(HERE, "libspeedy_b200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
-# The forward kernels (speedy_ensemble.cu) divide with the hardware's approximate division and
-# flush subnormal results to zero: they are bound by instruction issue, and IEEE division and
-# subnormal handling cost several instructions each (measured: the ragged-ensemble step 0.231 ->
-# 0.207 ms).  Tendencies, precipitation and diagnostics keep their measured distance to the
-# float32 and float64 oracles at the printed digits, with no new trigger flips; the only values
-# flushed are transmissivities below 1e-38.  The adjoint keeps IEEE arithmetic.
-SOURCE_FLAGS = {"csrc/speedy_ensemble.cu": ["-prec-div=false", "-ftz=true"]}
+# The forward kernels (speedy_ensemble.cu) are compiled without multiply-add contraction
+# (-fmad=false): the reference's float32 arithmetic (XLA without fast-math, like NumPy) rounds
+# every product and every sum, and contraction was the main source of the forward's elementwise
+# distance to it (measured at T425: humidity tendency 7.2e-6 -> 2.8e-6 and convective
+# precipitation 6.7e-6 -> 2.4e-6 of their maxima, wind tendencies 1e-6 -> 1.5e-8, downward
+# shortwave 2.1e-4 -> 4.5e-5; it costs about 5 % of the forward's time).  They divide with the
+# hardware's approximate division and flush subnormal results to zero: the forward is bound by
+# instruction issue, IEEE division and subnormal handling cost several instructions each, and
+# measured against the oracles they change nothing (tendencies, precipitation and diagnostics
+# keep their distances at the printed digits; the only values flushed are transmissivities below
+# 1e-38).  The adjoint keeps IEEE arithmetic.
+SOURCE_FLAGS = {"csrc/speedy_ensemble.cu": ["-fmad=false", "-prec-div=false", "-ftz=true"]}
 
 
 def _nvcc():

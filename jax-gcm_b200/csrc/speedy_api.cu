@@ -36,7 +36,8 @@ bool overlap(const Span& a, const Span& b) { return a.lo < b.hi && b.lo < a.hi; 
 // True when an output field overlaps an input field or another output field.
 static bool outputs_alias(const spd_desc_t* d, const spd_inputs_t* in, const spd_outputs_t* out) {
   const size_t C = (size_t)d->ix * d->il, L = (size_t)d->kx * C;
-  const Span ins[] = {span(in->u_wind, L), span(in->v_wind, L), span(in->temperature, L),
+  const size_t W = (d->flags & SPD_LOW_LEVEL_WINDS) ? C : L;  // wind planes
+  const Span ins[] = {span(in->u_wind, W), span(in->v_wind, W), span(in->temperature, L),
                       span(in->specific_humidity, L), span(in->geopotential, L),
                       span(in->normalized_surface_pressure, C), span(in->alb0, C),
                       span(in->sice_am, C), span(in->snowc_am, C), span(in->soilw_am, C),
@@ -48,8 +49,8 @@ static bool outputs_alias(const spd_desc_t* d, const spd_inputs_t* in, const spd
                          out->tskin, out->shf, out->evap};
   Span outs[6 + 13 + 2];
   int n = 0;
-  outs[n++] = span(out->u_wind, L);
-  outs[n++] = span(out->v_wind, L);
+  outs[n++] = span(out->u_wind, W);
+  outs[n++] = span(out->v_wind, W);
   outs[n++] = span(out->temperature, L);
   outs[n++] = span(out->specific_humidity, L);
   outs[n++] = span(out->precnv, C);
@@ -85,7 +86,7 @@ int check_instance(const spd_desc_t* d, const spd_inputs_t* in, const spd_output
 }
 
 // check_instance plus the forward's own rule: its outputs overlap neither its inputs nor one
-// another (the first launch stages values in the output planes that the second reads back).
+// another (a column's outputs are written while other columns still read their inputs).
 int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
                            const spd_outputs_t* out) {
   const int rc = check_instance(d, in, out);

@@ -14,10 +14,12 @@
 // absorbed fluxes are added to the temperature accumulator as each piece completes, and the
 // vertical-diffusion terms are formed level by level in one ascending pass.
 //
-// The column is split in two halves, run by two launches: column_first (humidity through
-// clouds) ends at the cloud-top level, the one cross-column dependency; column_second
-// (radiation, surface fluxes, vertical diffusion) needs the instance's level set of cloud tops
-// and resumes from what the first half left (qsat, the tendency accumulators, a few scalars).
+// The column is written in two halves: column_first (humidity through clouds) ends at the
+// cloud-top level, the one cross-column dependency; column_second (radiation, surface fluxes,
+// vertical diffusion) needs the instance's level set of cloud tops and resumes from what the
+// first half left (qsat, the tendency accumulators, a few scalars).  The forward runs both in
+// one launch (speedy_kernels.cuh, fused_process) after a light launch that forms the level set
+// from column_first<KX, true>.
 //
 // Expression order follows the reference term by term (file:line relative to the JAX-GCM
 // root).  Deviations, all at the rounding level and never inside a cancelling difference:
@@ -121,7 +123,10 @@ __device__ __forceinline__ void radset_w(float temp, float w, float fb[4]) {
 // Q (clamped by the caller where verify applies), PHI, and s.psa, s.fmask.  Out: qsat QS, the
 // convective + condensation tendency accumulators DT and DQ, and in o the convective and
 // cloud results (iptop, icltop, cbmf, precnv, precls, cloudc, clstr).
-template <int KX>
+// kTopOnly: only o.icltop (and o.iptop), from the same expressions, skipping the tendencies,
+// precipitation and cloud cover -- the level-set launch, whose S must agree bit for bit with the
+// cloud tops the full first half finds.
+template <int KX, bool kTopOnly = false>
 __device__ __forceinline__ void column_first(const ConstsD& C, const float (&T)[KX],
                                              const float (&Q)[KX], const float (&PHI)[KX],
                                              const SurfaceIn& s, float (&QS)[KX],
@@ -178,7 +183,7 @@ __device__ __forceinline__ void column_first(const ConstsD& C, const float (&T)[
   }
 
   // ---- get_convection_tendencies (convection.py:99-237) -----------------------------------
-  {
+  if constexpr (!kTopOnly) {
     const bool mask = iptop < KX;
     const float qmax = fmaxf(1.01f * q_b, QS[KX - 1]);
     const float w_last = vg.wvi[KX - 2][1];
@@ -277,11 +282,13 @@ __device__ __forceinline__ void column_first(const ConstsD& C, const float (&T)[
         dtl = tfact * fminf(-dql, D.dqmax[k] * psa2);
         if (first == 0) first = k;
       }
-      DT[k] = DT[k] + dtl;
-      DQ[k] = DQ[k] + dql;
-      psum = psum + D.pfact[k] * dql;
+      if constexpr (!kTopOnly) {
+        DT[k] = DT[k] + dtl;
+        DQ[k] = DQ[k] + dql;
+        psum = psum + D.pfact[k] * dql;
+      }
     }
-    o.precls = (0.0f - psum) * psa;
+    if constexpr (!kTopOnly) o.precls = (0.0f - psum) * psa;
     iptop = min(first == 0 ? 1 : first, iptop);
   }
   o.iptop = iptop;
@@ -310,6 +317,10 @@ __device__ __forceinline__ void column_first(const ConstsD& C, const float (&T)[
       allm = allm && m;
     }
     const int icl = (allm && cmin == cmax) ? KX - 3 : icl0;
+    if constexpr (kTopOnly) {
+      o.icltop = min(iptop, icl);
+      return;
+    }
     const float gse = (se_b1 - se_b) / (PHI[KX - 2] - PHI[KX - 1]);
     const float pr1 = fminf(p.pmaxcl, 86.4f * (o.precnv + o.precls));
     cloudc = fminf(1.0f, p.wpcl * sqrtf(fmaxf(kEpsilon, pr1)) + sq(fminf(1.0f, cmax * D.rrcl)));

@@ -4,12 +4,12 @@
 // A member is one grid instance (its own arrays, ix*il columns, kx levels).  The plan splits
 // every member into tiles of kNT consecutive columns (a tile never straddles members), ordered
 // by level count (16-level tiles first, the heavier work), and keeps per member the field
-// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 runs the
-// first half of every column on all tiles (each member's level set, solar table and staged
-// values, as in spd_fwd's first launch); launch 2 runs the second half on all tiles, reading
-// each member's level set.  Both launches are persistent: gridDim blocks stride over the tile
-// list.  The plain per-instance forward (spd_fwd) runs the same two kernels over a one-member
-// plan given by value, so that the two paths agree bitwise.
+// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 (light)
+// forms each member's level set S and solar table from the cloud-top part of every column;
+// launch 2 runs every column whole, in one pass, reading its member's S (the one cross-column
+// dependency, shortwave_radiation.py:62-68) and solar table.  Both launches are persistent:
+// gridDim blocks stride over the tile list.  The plain per-instance forward (spd_fwd) runs the
+// same two kernels over a one-member plan given by value, so that the two paths agree bitwise.
 // Constants shared by a class of members (kx, date, switches, vertical grid, parameters) travel
 // by value in the kernel parameters.
 #include <cuda_runtime.h>
@@ -28,21 +28,20 @@ int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
                            const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 
-// Rows the first launch reads for a tile of member m: T, q, phi at every level, psa, fmask.
-__device__ __forceinline__ void prefetch_moist_tile(const MemberDev& m, int col0) {
+// Rows the level-set launch reads for a tile of member m: T, q, phi at every level, psa.
+__device__ __forceinline__ void prefetch_levelset_tile(const MemberDev& m, int col0) {
   const int kx = m.kx;
   const size_t C = m.C;
-  prefetch_tile_rows(3 * kx + 2, [&](int r) -> const float* {
+  prefetch_tile_rows(3 * kx + 1, [&](int r) -> const float* {
     if (r < kx) return m.in.temperature + r * C + col0;
     if (r < 2 * kx) return m.in.specific_humidity + (r - kx) * C + col0;
     if (r < 3 * kx) return m.in.geopotential + (r - 2 * kx) * C + col0;
-    return (r == 3 * kx ? m.in.normalized_surface_pressure : m.in.fmask) + col0;
+    return m.in.normalized_surface_pressure + col0;
   });
 }
 
 // The tile this block processes `stride` tiles ahead, if it is a full tile: its rows are
-// prefetched into L2 while the current tile computes (first launch only: in the second launch
-// the prefetches cost more than they saved, 0.139 -> 0.149 ms on the ragged ensemble).
+// prefetched into L2 while the current tile computes.
 template <class F>
 __device__ __forceinline__ void prefetch_ahead(const TileSource& T, int t, int stride, int ntiles,
                                                F prefetch) {
@@ -53,10 +52,12 @@ __device__ __forceinline__ void prefetch_ahead(const TileSource& T, int t, int s
   if (mn.C - col0n >= kNT) prefetch(mn, col0n);
 }
 
-__global__ void __launch_bounds__(kNT, 5) ensemble_moist(const __grid_constant__ ClassArgs A,
-                                                         const __grid_constant__ TileSource T,
-                                                         int ntiles, int pf_stride) {
-  // the second launch may start as this one's blocks retire (it waits for completion before
+// Launch 1: every member's per-latitude solar table and cloud-top level set S (an OR over its
+// columns' clipped cloud tops, formed by the first half's top-only form).
+__global__ void __launch_bounds__(kNT, 5) ensemble_levelset(const __grid_constant__ ClassArgs A,
+                                                            const __grid_constant__ TileSource T,
+                                                            int ntiles, int pf_stride) {
+  // the fused launch may start as this one's blocks retire (it waits for completion before
   // reading anything written here)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -64,23 +65,24 @@ __global__ void __launch_bounds__(kNT, 5) ensemble_moist(const __grid_constant__
     const MemberDev m = tile_member(T, t, col0);
     const int c = col0 + threadIdx.x;
     const ConstsD& CD = A.cls[m.cls];
-    prefetch_ahead(T, t, pf_stride, ntiles, prefetch_moist_tile);
+    prefetch_ahead(T, t, pf_stride, ntiles, prefetch_levelset_tile);
     if (c < m.il) m.table[c] = zonal_row(CD.K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
     uint32_t bit = 0;
     if (c < m.C) {
       switch (m.kx) {  // uniform per block
-        case 16: bit = first_process<16>(CD, m.in, m.out, c, m.C); break;
-        case 8: bit = first_process<8>(CD, m.in, m.out, c, m.C); break;
-        default: bit = first_process<7>(CD, m.in, m.out, c, m.C); break;
+        case 16: bit = levelset_bit<16>(CD, m.in, c, m.C); break;
+        case 8: bit = levelset_bit<8>(CD, m.in, c, m.C); break;
+        default: bit = levelset_bit<7>(CD, m.in, c, m.C); break;
       }
     }
     or_level_set(bit, m.S);
   }
 }
 
-__global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant__ ClassArgs A,
-                                                           const __grid_constant__ TileSource T,
-                                                           int ntiles) {
+// Launch 2: every column whole (fused_process), reading its member's S and solar table.
+__global__ void __launch_bounds__(kNT, 4) ensemble_fused(const __grid_constant__ ClassArgs A,
+                                                         const __grid_constant__ TileSource T,
+                                                         int ntiles) {
   extern __shared__ float sm[];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     int col0;
@@ -89,9 +91,9 @@ __global__ void __launch_bounds__(kNT, 4) ensemble_columns(const __grid_constant
     if (c < m.C) {
       const ConstsD& CD = A.cls[m.cls];
       switch (m.kx) {
-        case 16: column_process<16>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
-        case 8: column_process<8>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
-        default: column_process<7>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
+        case 16: fused_process<16>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
+        case 8: fused_process<8>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
+        default: fused_process<7>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
       }
     }
   }
@@ -101,7 +103,8 @@ static size_t arena_bytes(int kx) { return (size_t)kNumArrays * kx * kNT * sizeo
 
 namespace {
 struct Residency {
-  int sms = 0, moist = 0, cols[17] = {};  // resident blocks per SM; cols by arena level count
+  int sms = 0, lvl = 0, cols[17] = {};  // resident blocks per SM (level-set launch;
+                                          // fused launch by arena level count)
 };
 
 // SMs and resident blocks per SM of both kernels on the current device, set up once per device
@@ -116,17 +119,17 @@ int residency(Residency& R) {
   std::lock_guard<std::mutex> lock(mu);
   if (!done[dev]) {
     Residency r;
-    if (cudaFuncSetAttribute(ensemble_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(ensemble_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes<16>()) != cudaSuccess ||
         cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.moist, ensemble_moist, kNT, 0) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.lvl, ensemble_levelset, kNT, 0) !=
             cudaSuccess)
       return SPD_ERR_CUDA;
     for (int kx : {7, 8, 16})
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.cols[kx], ensemble_columns, kNT,
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.cols[kx], ensemble_fused, kNT,
                                                         arena_bytes(kx)) != cudaSuccess)
         return SPD_ERR_CUDA;
-    r.moist = std::max(r.moist, 1);
+    r.lvl = std::max(r.lvl, 1);
     for (int kx : {7, 8, 16}) r.cols[kx] = std::max(r.cols[kx], 1);
     cached[dev] = r;
     done[dev] = true;
@@ -141,22 +144,22 @@ int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_l
   Residency R;
   const int rc = residency(R);
   if (rc != SPD_OK) return rc;
-  const int res_moist = R.sms * R.moist, res_cols = R.sms * R.cols[kx_layout];
-  int grid_moist, grid_cols, pf_moist;
+  const int res_lvl = R.sms * R.lvl, res_cols = R.sms * R.cols[kx_layout];
+  int grid_lvl, grid_cols, pf_lvl;
   if (grid_blocks == SPD_GRID_PER_TILE) {
     // one block per tile; the blocks resident beside this one run the next wave, so the tile
     // a wave ahead is the one to prefetch
-    grid_moist = grid_cols = ntiles;
-    pf_moist = res_moist;
+    grid_lvl = grid_cols = ntiles;
+    pf_lvl = res_lvl;
   } else {
-    grid_moist = std::min(res_moist, ntiles);
+    grid_lvl = std::min(res_lvl, ntiles);
     grid_cols = std::min(grid_blocks > 0 ? grid_blocks : res_cols, ntiles);
-    pf_moist = grid_moist;
+    pf_lvl = grid_lvl;
   }
-  ensemble_moist<<<grid_moist, kNT, 0, st>>>(A, T, ntiles, pf_moist);
+  ensemble_levelset<<<grid_lvl, kNT, 0, st>>>(A, T, ntiles, pf_lvl);
   if (marker) {  // timing hook: the two launches apart, in plain stream order
     if (cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
-    ensemble_columns<<<grid_cols, kNT, arena_bytes(kx_layout), st>>>(A, T, ntiles);
+    ensemble_fused<<<grid_cols, kNT, arena_bytes(kx_layout), st>>>(A, T, ntiles);
     return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
   }
   // programmatic dependent launch: the second launch's blocks take SMs as the first launch's
@@ -171,14 +174,14 @@ int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_l
   cfg.stream = st;
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
-  if (cudaLaunchKernelEx(&cfg, ensemble_columns, A, T, ntiles) != cudaSuccess) return SPD_ERR_CUDA;
+  if (cudaLaunchKernelEx(&cfg, ensemble_fused, A, T, ntiles) != cudaSuccess) return SPD_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
 int preload_ensemble() {
   cudaFuncAttributes a;
-  bool ok = cudaFuncGetAttributes(&a, ensemble_moist) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, ensemble_columns) == cudaSuccess;
+  bool ok = cudaFuncGetAttributes(&a, ensemble_levelset) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_fused) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 

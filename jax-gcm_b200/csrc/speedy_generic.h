@@ -4,10 +4,10 @@
 // (jcm/physics/speedy/speedy_physics.py:88-127) for one column, term by term in the reference's
 // order, with the differentiable quantities (state, the 12 tuning parameters and everything
 // derived from them) of type R and the non-differentiated constants of type F.  With
-// R = spdad::Adj<F> it records the reverse-mode tape of the column; that is how the adjoint
-// kernel (speedy_adjoint.cu) recomputes the forward inside each column instead of storing it.
-// The same source compiles for the host (R = double or Adj<double>), which the tests use for
-// float64 finite-difference checks.
+// R = spdad::Adj<F> it records the reverse-mode tape of the column (speedy_ad.h).  Its users are
+// host builds: the tests' float32/float64 forward, the taped float64 VJP that checks the
+// device's hand-written reverse pass (speedy_vjp.h), and the compiled CPU restatement of the
+// reference (oracle/cpu_port.cpp, R = F = float) that the benchmark times as its CPU baseline.
 //
 // Each block cites the reference lines it restates (paths relative to the JAX-GCM root).  The
 // shortwave cloud-top level set S of the instance (shortwave_radiation.py:62-68) is an input.
@@ -81,7 +81,8 @@ SPD_HD void radset_r(const R& temp, F epslw, R fb[4]) {
 template <int KX, class R, class F>
 SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const DiffParams<R>& g,
                            uint32_t flags, int model_step, F ablco2, uint32_t S,
-                           const ColumnIn<R, F>& in, ColumnOut<R>& o) {
+                           const ColumnIn<R, F>& in, ColumnOut<R>& o,
+                           bool through_clouds_only = false) {
   const R psa = in.psa;
   const R* t = in.t;
   const R* q = in.q;
@@ -295,6 +296,9 @@ SPD_HD void column_generic(const spd_vgrid_t& vg, const spd_params_t& p, const D
   }
   o.cloudc = cloudc;
   o.icltop = icltop;
+  // The cloud-top level set S of the instance needs every column's icltop: a caller that
+  // forms S itself runs the terms up to here first (through_clouds_only), then the column.
+  if (through_clouds_only) return;
 
   // ---- shortwave_rad_fluxes (shortwave_radiation.py:27-217) ----
   R flux_sw0, flux_sw1, rsds;

@@ -51,44 +51,11 @@ __device__ __forceinline__ uint32_t prepass_column(const Consts& K, const spd_in
   return 1u << min(max(icl, 0), KX - 1);
 }
 
-// Where the first launch leaves its results for the second, in the call's own output planes
-// (the second launch rewrites every one of them): per level, the temperature and humidity
-// tendency accumulators in out.temperature and out.specific_humidity and qsat in out.u_wind;
-// per column, the scalars below in the first levels of out.v_wind (iptop and icltop as int
-// bit patterns).  The two precipitation fields are final after the first half and go straight
-// to their outputs.
-enum { ST_CBMF, ST_CLOUDC, ST_CLSTR, ST_IPTOP, ST_ICLTOP, kStagedScalars };
-static_assert(kStagedScalars <= 7, "the staged scalars fit the smallest level count");
-
-// Loads the column's T, q (clamped at zero under SPD_FUSE_VERIFY) and phi into shared memory;
-// returns the levels whose q was clamped.
+// Cloud-top level bit of column c, 1 << clip(icltop, 0, kx-1), from the forward's own first
+// half in its top-only form (the level-set launch).
 template <int KX>
-__device__ __forceinline__ uint32_t load_state(float* sm, const spd_inputs_t& in, bool verify,
-                                               int c, int C) {
-  float* tp = sm + (size_t)A_T * KX * kNT + threadIdx.x;
-  float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
-  float* pp = sm + (size_t)A_PHI * KX * kNT + threadIdx.x;
-  uint32_t neg = 0;
-#pragma unroll 4
-  for (int k = 0; k < KX; ++k) {
-    const size_t i = (size_t)k * C + c;
-    tp[k * kNT] = __ldg(in.temperature + i);
-    float q = __ldg(in.specific_humidity + i);
-    if (verify && q < 0.0f) {
-      neg |= 1u << k;
-      q = 0.0f;
-    }
-    qp[k * kNT] = q;
-    pp[k * kNT] = __ldg(in.geopotential + i);
-  }
-  return neg;
-}
-
-// First half of column c (humidity through clouds), in registers: stages its results and
-// returns the column's cloud-top level bit, 1 << clip(icltop, 0, kx-1).
-template <int KX>
-__device__ __forceinline__ uint32_t first_process(const ConstsD& CD, const spd_inputs_t& in,
-                                                  const spd_outputs_t& out, int c, int C) {
+__device__ __forceinline__ uint32_t levelset_bit(const ConstsD& CD, const spd_inputs_t& in,
+                                                 int c, int C) {
   const bool verify = (CD.K.flags & SPD_FUSE_VERIFY) != 0;
   float t[KX], q[KX], phi[KX];
 #pragma unroll
@@ -101,29 +68,10 @@ __device__ __forceinline__ uint32_t first_process(const ConstsD& CD, const spd_i
   }
   SurfaceIn s;
   s.psa = __ldg(in.normalized_surface_pressure + c);
-  s.fmask = __ldg(in.fmask + c);
+  s.fmask = 0.0f;
   float qs[KX], dt[KX], dq[KX];
   ColScalars o;
-  column_first<KX>(CD, t, q, phi, s, qs, dt, dq, o);
-#pragma unroll
-  for (int k = 0; k < KX; ++k) {
-    const size_t i = (size_t)k * C + c;
-    out.temperature[i] = dt[k];
-    out.specific_humidity[i] = dq[k];
-    out.u_wind[i] = qs[k];
-  }
-  out.v_wind[(size_t)ST_CBMF * C + c] = o.cbmf;
-  out.v_wind[(size_t)ST_CLOUDC * C + c] = o.cloudc;
-  out.v_wind[(size_t)ST_CLSTR * C + c] = o.clstr;
-  out.v_wind[(size_t)ST_IPTOP * C + c] = __int_as_float(o.iptop);
-  out.v_wind[(size_t)ST_ICLTOP * C + c] = __int_as_float(o.icltop);
-  if (CD.K.flags & SPD_ACCUMULATE_DIAGNOSTICS) {
-    out.precnv[c] = out.precnv[c] + o.precnv;
-    out.precls[c] = out.precls[c] + o.precls;
-  } else {
-    __stcs(out.precnv + c, o.precnv);
-    __stcs(out.precls + c, o.precls);
-  }
+  column_first<KX, true>(CD, t, q, phi, s, qs, dt, dq, o);
   return 1u << min(max(o.icltop, 0), KX - 1);
 }
 
@@ -144,54 +92,19 @@ __device__ __forceinline__ void orographic_horizontal(const Derived& D, float ph
   qcorh = 0.7f * (qref - qsfc);  // refrh1 (physical_constants.py:27)
 }
 
-// Second half of column c: reloads the state and the first half's stage, runs radiation,
-// surface fluxes and vertical diffusion, applies verify_tendencies and stores every output.
-// `sm` is the block's shared-memory arena laid out for KX levels.
+// The end of column c, shared by the forward's kernels: the orographic correction (the last
+// term, when on), verify_tendencies, the tendency stores and the diagnostics.  The level arrays
+// T, Q (clamped by verify_state where `neg` has a bit), the accumulated tendencies DT and DQ are
+// in the block's shared-memory arena; o holds the column's scalar results.
 template <int KX>
-__device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
+__device__ __forceinline__ void column_outputs(const ConstsD& CD, float* sm,
                                                const spd_inputs_t& in, const spd_outputs_t& out,
-                                               const uint32_t* S,
-                                               const ZonalRow* __restrict__ table, int c, int C,
-                                               int il) {
+                                               const SurfaceIn& s, const ColScalars& o,
+                                               uint32_t neg, int c, int C) {
   const Consts& K = CD.K;
   const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
-  const uint32_t neg = load_state<KX>(sm, in, verify, c, C);
-  // Everything below reads the first launch's results (stage, level set, solar table).  When
-  // this launch overlaps the first one's tail (programmatic dependent launch), wait here for
-  // its completion; otherwise the first launch is complete already and this returns at once.
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  const uint32_t Sw = *S;
-  float* qsp = sm + (size_t)A_QSAT * KX * kNT + threadIdx.x;
   float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
   float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
-#pragma unroll 4
-  for (int k = 0; k < KX; ++k) {
-    const size_t i = (size_t)k * C + c;
-    dtp[k * kNT] = __ldcs(out.temperature + i);
-    dqp[k * kNT] = __ldcs(out.specific_humidity + i);
-    qsp[k * kNT] = __ldcs(out.u_wind + i);
-  }
-  ColScalars o;
-  o.cbmf = __ldcs(out.v_wind + (size_t)ST_CBMF * C + c);
-  o.cloudc = __ldcs(out.v_wind + (size_t)ST_CLOUDC * C + c);
-  o.clstr = __ldcs(out.v_wind + (size_t)ST_CLSTR * C + c);
-  o.iptop = __float_as_int(__ldcs(out.v_wind + (size_t)ST_IPTOP * C + c));
-  o.icltop = __float_as_int(__ldcs(out.v_wind + (size_t)ST_ICLTOP * C + c));
-  SurfaceIn s;
-  s.psa = __ldg(in.normalized_surface_pressure + c);
-  s.u_low = __ldg(in.u_wind + (size_t)(KX - 1) * C + c);
-  s.v_low = __ldg(in.v_wind + (size_t)(KX - 1) * C + c);
-  s.sst = __ldg(in.sea_surface_temperature + c);
-  s.stl = __ldg(in.stl_am + c);
-  s.soilw = __ldg(in.soilw_am + c);
-  s.snowc = __ldg(in.snowc_am + c);
-  s.sice = __ldg(in.sice_am + c);
-  s.alb0 = __ldg(in.alb0 + c);
-  s.fmask = __ldg(in.fmask + c);
-  s.orog = __ldg(in.orog + c);
-  s.phis0 = __ldg(in.phis0 + c);
-  const ZonalRow z = table[c % il];
-  column_second<KX>(CD, sm, s, z, Sw, o);
   if (K.flags & SPD_OROGRAPHIC) {  // the last term (get_orographic_correction_tendencies)
     float tcorh, qcorh;
     orographic_horizontal(CD.D, s.phis0, s.fmask, s.stl, s.sst, tcorh, qcorh);
@@ -215,20 +128,34 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
     }
   }
   const float qs = K.q_tend_scale;
+  const bool low = (K.flags & SPD_LOW_LEVEL_WINDS) != 0;
 #pragma unroll 4
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
-    __stcs(out.u_wind + i, k == KX - 1 ? o.du_low : 0.0f);
-    __stcs(out.v_wind + i, k == KX - 1 ? o.dv_low : 0.0f);
+    if (!low) {
+      __stcs(out.u_wind + i, k == KX - 1 ? o.du_low : 0.0f);
+      __stcs(out.v_wind + i, k == KX - 1 ? o.dv_low : 0.0f);
+    }
     __stcs(out.temperature + i, dtp[k * kNT]);
     const float dq = dqp[k * kNT];
     __stcs(out.specific_humidity + i, qs != 1.0f ? dq * qs : dq);
+  }
+  if (low) {  // the lowest level only: single planes
+    __stcs(out.u_wind + c, o.du_low);
+    __stcs(out.v_wind + c, o.dv_low);
   }
   // diagnostics: stored, or added to the caller's sums under SPD_ACCUMULATE_DIAGNOSTICS
   const bool acc = (K.flags & SPD_ACCUMULATE_DIAGNOSTICS) != 0;
   auto put = [&](float* f, float x) {
     if (f) f[c] = acc ? f[c] + x : x;
   };
+  if (acc) {
+    out.precnv[c] = out.precnv[c] + o.precnv;
+    out.precls[c] = out.precls[c] + o.precls;
+  } else {
+    __stcs(out.precnv + c, o.precnv);
+    __stcs(out.precls + c, o.precls);
+  }
   put(out.cbmf, o.cbmf);
   put(out.cloudc, o.cloudc);
   put(out.cloudstr, o.clstr);
@@ -244,6 +171,74 @@ __device__ __forceinline__ void column_process(const ConstsD& CD, float* sm,
   put(out.evap, o.evap);
   if (out.iptop) out.iptop[c] = o.iptop;
   if (out.icltop) out.icltop[c] = o.icltop;
+}
+
+// The whole column c in one pass: the first half (humidity through clouds) with its level
+// arrays in registers, its results and the state moved into the block's shared-memory arena,
+// then the second half (radiation, surface fluxes, vertical diffusion) and the outputs.  The
+// instance's cloud-top level set *S and its per-latitude solar table come from the level-set
+// launch before this one; they are read only after the first half, behind griddepcontrol.wait
+// (when this launch overlaps that one's tail, it waits there for that launch's completion;
+// otherwise it returns at once).
+template <int KX>
+__device__ __forceinline__ void fused_process(const ConstsD& CD, float* sm,
+                                              const spd_inputs_t& in, const spd_outputs_t& out,
+                                              const uint32_t* S,
+                                              const ZonalRow* __restrict__ table, int c, int C,
+                                              int il) {
+  const Consts& K = CD.K;
+  const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
+  const bool low = (K.flags & SPD_LOW_LEVEL_WINDS) != 0;
+  float t[KX], q[KX], phi[KX];
+  uint32_t neg = 0;
+#pragma unroll
+  for (int k = 0; k < KX; ++k) {
+    const size_t i = (size_t)k * C + c;
+    t[k] = __ldg(in.temperature + i);
+    const float qk = __ldg(in.specific_humidity + i);
+    if (verify && qk < 0.0f) neg |= 1u << k;
+    q[k] = (verify && qk < 0.0f) ? 0.0f : qk;
+    phi[k] = __ldg(in.geopotential + i);
+  }
+  SurfaceIn s;
+  s.psa = __ldg(in.normalized_surface_pressure + c);
+  s.fmask = __ldg(in.fmask + c);
+  ColScalars o;
+  {
+    float qs[KX], dt[KX], dq[KX];
+    column_first<KX>(CD, t, q, phi, s, qs, dt, dq, o);
+    float* tp = sm + (size_t)A_T * KX * kNT + threadIdx.x;
+    float* qp = sm + (size_t)A_Q * KX * kNT + threadIdx.x;
+    float* pp = sm + (size_t)A_PHI * KX * kNT + threadIdx.x;
+    float* qsp = sm + (size_t)A_QSAT * KX * kNT + threadIdx.x;
+    float* dtp = sm + (size_t)A_DT * KX * kNT + threadIdx.x;
+    float* dqp = sm + (size_t)A_DQ * KX * kNT + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < KX; ++k) {
+      tp[k * kNT] = t[k];
+      qp[k * kNT] = q[k];
+      pp[k * kNT] = phi[k];
+      qsp[k * kNT] = qs[k];
+      dtp[k * kNT] = dt[k];
+      dqp[k * kNT] = dq[k];
+    }
+  }
+  const size_t lw = low ? 0 : (size_t)(KX - 1) * C;
+  s.u_low = __ldg(in.u_wind + lw + c);
+  s.v_low = __ldg(in.v_wind + lw + c);
+  s.sst = __ldg(in.sea_surface_temperature + c);
+  s.stl = __ldg(in.stl_am + c);
+  s.soilw = __ldg(in.soilw_am + c);
+  s.snowc = __ldg(in.snowc_am + c);
+  s.sice = __ldg(in.sice_am + c);
+  s.alb0 = __ldg(in.alb0 + c);
+  s.orog = __ldg(in.orog + c);
+  s.phis0 = __ldg(in.phis0 + c);
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const uint32_t Sw = *S;
+  const ZonalRow z = table[c % il];
+  column_second<KX>(CD, sm, s, z, Sw, o);
+  column_outputs<KX>(CD, sm, in, out, s, o, neg, c, C);
 }
 
 }  // namespace spd

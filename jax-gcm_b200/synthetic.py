@@ -203,22 +203,22 @@ def t425_instance(seed=425, kx=16):
     return inst
 
 
+def path_bytes(kx, columns):
+    """Algorithmic bytes of one forward call: u, v, T, q and phi at every level, psa, six
+    forcing and three geometry fields read; four tendency planes and the two precipitation
+    fields written, each once: 4 (9 kx + 12) bytes per column."""
+    return 4 * (9 * kx + 12) * columns
+
+
 def fwd_bytes(kx, columns):
-    """Minimum bytes a forward call must move: T, q, phi at every level, u and v at the lowest
-    level, psa, six forcing fields and three geometry fields read; four tendency planes and two
-    precipitation fields written."""
+    """Bytes a forward call must move at least: T, q, phi at every level, u and v at the lowest
+    level (the only level the physics reads), psa, six forcing and three geometry fields read;
+    four tendency planes and two precipitation fields written: 4 (7 kx + 14) bytes per
+    column."""
     return 4 * (7 * kx + 14) * columns
 
 
-def first_half_bytes(kx, columns):
-    """Bytes the forward's first launch must move: T, q, phi at every level, psa and fmask read;
-    the staged temperature and humidity accumulators and qsat at every level, five staged
-    scalars and the two precipitation fields written."""
-    return 4 * (6 * kx + 9) * columns
-
-
-def second_half_bytes(kx, columns):
-    """Bytes the forward's second launch must move: T, q, phi and the three staged level fields
-    at every level, the five staged scalars, psa, the lowest u and v, six forcing and three
-    geometry fields read; the four tendency planes written."""
-    return 4 * (10 * kx + 17) * columns
+def levelset_bytes(kx, columns):
+    """Bytes the forward's level-set launch reads: T, q, phi at every level and psa,
+    4 (3 kx + 1) per column (a re-read of the fused launch's inputs)."""
+    return 4 * (3 * kx + 1) * columns

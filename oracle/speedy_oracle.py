@@ -285,6 +285,10 @@ def dcopy(x):
 class Margins:
     """Records, per column, the smallest distance (in float32 ulps) of any threshold test.
 
+    A test is recorded between the two quantities it compares, on their own scale (a difference
+    tested against zero is recorded between the terms it subtracts), so that the distance in
+    ulps says how much rounding it takes to decide the test the other way.
+
     Columns whose CUDA result differs from the oracle beyond tolerance must have a trigger
     within a few ulps of its threshold (a "trigger flip"); the parity tests count them.
     """
@@ -295,8 +299,10 @@ class Margins:
     def cmp(self, a, b):
         a = np.asarray(a, np.float64)
         b = np.asarray(b, np.float64)
-        scale = np.maximum(np.maximum(np.abs(a), np.abs(b)), 1e-30)
-        u = np.abs(a - b) / (scale * 2.0 ** -23)
+        scale = np.maximum(np.abs(a), np.abs(b))
+        with np.errstate(all="ignore"):
+            u = np.abs(a - b) / (scale * 2.0 ** -23)
+        u = np.where(scale == 0.0, np.inf, u)  # 0 against 0: both sides exact, no threshold
         while u.ndim > len(self.ulps.shape):
             u = u.min(axis=0)
         u = np.broadcast_to(u, self.ulps.shape)
@@ -629,7 +635,7 @@ def clouds(state, data, params, forcing, geometry, rec=None):
     cloudc = np.where(mask, rh[nl1] - ps.rhcl1, 0.0)
     icltop = np.where(mask, nl1, nlp)
     drh = rh[2:kx - 2] - ps.rhcl1
-    _rec(rec, drh, cloudc[None])
+    _rec(rec, rh[2:kx - 2], (cloudc + ps.rhcl1)[None])  # drh > cloudc, on the scale of rh
     _rec(rec, state.specific_humidity[2:kx - 2], ps.qacl)
     m = (drh > cloudc) & (state.specific_humidity[2:kx - 2] > ps.qacl)
     cloudc_update = np.where(m, drh, cloudc)
@@ -973,7 +979,8 @@ def get_surface_fluxes(state, data, params, forcing, geometry, rec=None):
             hfluxn[:, :, 0] = hfluxn[:, :, 0] - (clamb * (tskin - stl_am))
             dtskin = tskin + 1.0
             qsat0[:, :, 1] = get_qsat(dtskin, psa, 1.0, rec)
-            _rec(rec, evap[:, :, 0], 0.0)
+            # evap > 0: the sign of soilw qsat0 - q1 under the max(0, .) above
+            _rec(rec, forcing.soilw_am * qsat0[:, :, 0], q1[:, :, 0])
             qsat0[:, :, 1] = np.where(evap[:, :, 0] > 0.0,
                                       forcing.soilw_am * (qsat0[:, :, 1] - qsat0[:, :, 0]), 0.0)
             with np.errstate(all="ignore"):
@@ -1052,9 +1059,10 @@ def get_vertical_diffusion_tend(state, data, params, forcing, geometry, rec=None
     fvdiq2 = fvdiq * hsg[nl1]
     dmse = se[kx - 1] - se[nl1 - 1] + ALHC * (qa[kx - 1] - qsat[nl1 - 1])
     drh = rh[kx - 1] - rh[nl1 - 1]
-    _rec(rec, dmse, 0.0)
-    _rec(rec, drh, 0.0)
-    _rec(rec, drh, drh0)
+    # dmse >= 0, drh >= 0 and drh >= drh0, each between the quantities the differences cancel
+    _rec(rec, se[kx - 1] + ALHC * qa[kx - 1], se[nl1 - 1] + ALHC * qsat[nl1 - 1])
+    _rec(rec, rh[kx - 1], rh[nl1 - 1])
+    _rec(rec, rh[kx - 1], rh[nl1 - 1] + drh0)
     fcnv = np.ones((ix, il), dt_)
     fcnv = np.where(np.logical_and(icnv > 0, dmse >= 0), pv.redshc, fcnv)
     fluxse = np.where(dmse >= 0.0, fcnv * fshcse * dmse, 0)
@@ -1073,7 +1081,7 @@ def get_vertical_diffusion_tend(state, data, params, forcing, geometry, rec=None
     drh0v = pv.rhgrad * (fsg[kr + 1] - fsg[kr])
     fvdiq2v = fvdiq * hsg[kr + 1]
     drhv = rh[kr + 1] - rh[kr]
-    _rec(rec, drhv, drh0v[:, None, None])
+    _rec(rec, rh[kr + 1], rh[kr] + drh0v[:, None, None])  # drhv >= drh0v, on the scale of rh
     fluxq = np.where((drhv >= drh0v[:, None, None]) & cond[:, None, None],
                      fvdiq2v[:, None, None] * qsat[kr] * drhv, 0)
     qt[kr] = qt[kr] + fluxq * rsig[kr][:, None, None]

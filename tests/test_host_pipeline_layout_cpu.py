@@ -9,7 +9,7 @@ pkg = importlib.import_module("jax-gcm_b200")
 B = pkg.batched
 
 SHAPES = [(8, 64, 32), (16, 96, 48), (8, 3, 5), (16, 512, 256), (7, 1, 1)]
-LEVEL = {"u_wind", "v_wind", "temperature", "specific_humidity", "geopotential"}
+LEVEL = {"temperature", "specific_humidity", "geopotential"}  # winds: lowest level only
 
 
 def members():
