@@ -42,7 +42,10 @@ SIGMA_LAYER_BOUNDARIES = {
 def _dev(x, device, dtype=torch.float32):
     if isinstance(x, torch.Tensor):
         return x.to(device=device, dtype=dtype).contiguous()
-    return torch.as_tensor(np.asarray(x), dtype=dtype, device=device).contiguous()
+    a = np.asarray(x)
+    if not a.flags.writeable:  # e.g. a broadcast view: torch wants its own writable copy
+        a = np.array(a)
+    return torch.as_tensor(a, dtype=dtype, device=device).contiguous()
 
 
 # ---------------------------------------------------------------------------------------------

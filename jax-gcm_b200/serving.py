@@ -7,9 +7,11 @@ under a cotangent the request seeds.  The reference has no serving layer; this m
 layer a forecast service would put in front of the physics:
 
 * Admission by free HBM.  Every device byte the loop holds (resident member state, result and
-  cotangent buffers, the adjoint's scratch) is counted against ``budget_bytes``.  A request is
-  admitted, in arrival order, when its new members and its result buffers fit; idle resident
-  members are evicted least-recently-used to make room.  A request that can never fit is
+  cotangent buffers, the adjoint's scratch) is counted against ``budget_bytes``, and a request
+  must also fit the device memory the backend can still hand out (its pool's free bytes plus
+  the driver's free memory, measured at admission).  A request is admitted, in arrival order,
+  when its new members and its result buffers fit; idle resident members are evicted
+  least-recently-used to make room.  A request that can never fit is
   rejected; a failed device allocation leaves the request waiting and is counted.
 * Device-resident column state.  A member's state, forcing and geometry are uploaded once, as
   one packed buffer from pinned host memory on a copy stream, and stay on the device while any
@@ -273,17 +275,26 @@ class Scheduler:
         return False
 
     # -- residency and admission ----------------------------------------------------------------
+    def _fits(self, nbytes):
+        """Within the budget, and within the device memory the backend can still hand out
+        (free HBM: its pool's free bytes plus what the driver reports free), when the backend
+        measures it."""
+        if self.budget - self.used < nbytes:
+            return False
+        avail = getattr(self.b, "available_bytes", None)
+        return avail is None or avail() >= nbytes
+
     def _evict_for(self, nbytes, keep):
         idle = sorted((r for r in self.resident.values() if r.refs == 0 and r.key not in keep),
                       key=lambda r: r.last_use)
         for r in idle:
-            if self.budget - self.used >= nbytes:
+            if self._fits(nbytes):
                 break
             self.b.release(r.dev)
             self.used -= self.b.member_bytes(r.host)
             del self.resident[r.key]
             self.stats["evictions"] += 1
-        return self.budget - self.used >= nbytes
+        return self._fits(nbytes)
 
     def _admit_one(self, req) -> bool:
         keys = list(dict.fromkeys(req.members))
@@ -767,6 +778,13 @@ class CudaBackend:
         dm = _DevMember(h, buf, inputs, ev)
         dm.handle = handle
         return dm
+
+    def available_bytes(self):
+        """Device bytes this backend can still hand out: its pool's free bytes, plus the
+        device's free memory (the pool grows into it), less a 1 GiB margin for the driver and
+        other users of the device."""
+        free, _ = self.torch.cuda.mem_get_info(self.dev)
+        return (self.arena.reserved - self.arena.in_use) + max(0, int(free) - (1 << 30))
 
     def release(self, dm):
         # The member's upload may still be running on the copy stream (a prefetched member, or

@@ -8,7 +8,7 @@ stores it under ``"<file>::<function>::<n>"``; the ``.npy`` arrays are stored un
 ``"npy::<name>"``.  The fixture is small and committed, because the reference tree is not
 available where the GPU tests run.
 
-Usage:  python tests/golden/make_golden.py [/path/to/jax-gcm]
+Usage:  python tests/golden/make_golden.py /path/to/jax-gcm
 """
 import ast
 import json
@@ -110,4 +110,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the JAX-GCM checkout>")
+    main(sys.argv[1])

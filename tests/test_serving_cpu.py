@@ -417,3 +417,43 @@ def test_cuda_backend_release_waits_for_the_upload_before_freeing():
     be.release(dm)
     assert order == ["upload done", ("arena release", 7)]
     assert dm.buf is None
+
+
+def test_admission_waits_for_free_device_memory_below_the_budget():
+    """A backend that measures its free device memory below what the budget would allow:
+    requests are admitted only as far as that memory goes (idle members evicted first), the
+    rest wait until memory frees up; the budget alone would have admitted both at once."""
+    class Measured(FakeBackend):
+        def __init__(self, limit, **kw):
+            super().__init__(**kw)
+            self.limit = limit
+            self.held = {}
+
+        def available_bytes(self):
+            return self.limit - sum(self.held.values())
+
+        def upload(self, h):
+            d = super().upload(h)
+            self.held[d] = h.nbytes
+            return d
+
+        def release(self, d):
+            self.held.pop(d, None)
+            return super().release(d)
+
+    out = 4 * (4 * 8 + 2) * 64 * 32
+    m = 10 * out
+    hosts = dict(a=host(8, 64, 32, nbytes=m), b=host(8, 64, 32, nbytes=m))
+    be = Measured(limit=m + 2 * out, per_col=1e-3)
+    sch = S.Scheduler(be, hosts.__getitem__, budget_bytes=1 << 40)
+    r0 = sch.submit(S.Request(S.TENDENCY, ["a"]))
+    r1 = sch.submit(S.Request(S.TENDENCY, ["b"]))
+    sch.step()
+    assert r0.status == "running" and r1.status == "waiting"
+    be.t = 100.0
+    sch.step()                            # r0 done: "a" evicted to make room for "b"
+    assert r0.status == "done" and r1.status in ("running", "done")
+    assert sch.stats["evictions"] == 1
+    be.t = 200.0
+    sch.step()
+    assert r1.status == "done"
