@@ -707,6 +707,7 @@ class CudaBackend:
         if reserve_bytes > 0:  # a service sizes its pool once, at startup
             self.arena.reserve(reserve_bytes)
         self.pinned = PinnedCache()
+        self._free_at, self._free_reserved, self._dev_free = None, None, 0
         self._t0 = None
         self._h0 = 0.0
 
@@ -782,9 +783,15 @@ class CudaBackend:
     def available_bytes(self):
         """Device bytes this backend can still hand out: its pool's free bytes, plus the
         device's free memory (the pool grows into it), less a 1 GiB margin for the driver and
-        other users of the device."""
-        free, _ = self.torch.cuda.mem_get_info(self.dev)
-        return (self.arena.reserved - self.arena.in_use) + max(0, int(free) - (1 << 30))
+        other users of the device.  The driver's figure is measured at most every half second
+        and after the pool grows (cudaMemGetInfo on every admission cost the request loop
+        milliseconds per request), the pool's own figure exactly."""
+        now = time.perf_counter()
+        if (self._free_at is None or now - self._free_at > 0.5 or
+                self._free_reserved != self.arena.reserved):
+            self._dev_free = int(self.torch.cuda.mem_get_info(self.dev)[0])
+            self._free_at, self._free_reserved = now, self.arena.reserved
+        return (self.arena.reserved - self.arena.in_use) + max(0, self._dev_free - (1 << 30))
 
     def release(self, dm):
         # The member's upload may still be running on the copy stream (a prefetched member, or

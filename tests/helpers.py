@@ -10,14 +10,18 @@ import numpy as np
 #
 # i.e. relative error RTOL = 1e-5 above a per-field absolute floor.  Integer levels (iptop,
 # icltop) must match exactly.  Columns outside the bar must be trigger flips: a threshold test
-# of that column sits within FLIP_ULPS float32 ulps of its threshold in the oracle (counted, in
-# ulp buckets, and bounded).  The floors are the float32 conditioning of each field: the
-# temperature and humidity tendencies are sums of radiative, convective and diffusive terms
-# that cancel, and two float32 evaluations of the reference arithmetic that differ only in the
-# last bits of their exponentials already disagree by more than 1e-5 relative at elements below
-# these floors (tests/test_float32_sensitivity.py measures this on the oracle alone).  The
-# winds and precipitation take the floor 1e-3.  Normwise error <= RTOL * max|f| is asserted as
-# a second line, and the CUDA path's error against the float64 oracle must stay within
+# of that column sits within FLIP_ULPS float32 ulps of its threshold in the oracle (counted by
+# ulp bucket -- within 1, within 4, within 64 -- and bounded).  The floors follow the float32
+# conditioning of each field.  The winds and the large-scale precipitation take 1e-3.  The
+# temperature and humidity tendencies and the convective precipitation are sums of radiative,
+# convective and diffusive terms that cancel: two float32 evaluations of the reference
+# arithmetic that differ only in the last bits of their exponentials already need floors of up
+# to 0.56 (temperature), 0.41 (humidity) and 0.36 (convective precipitation) of the field
+# maximum to agree within 1e-5 (tests/test_float32_sensitivity.py, and the same measurement on
+# the T425 instance), and the CUDA path needs at most 0.80, 0.48 and 0.41 over every GPU parity
+# case (T425 included); their floors are 1.0, 0.5 and 0.5 -- for the temperature tendency the
+# elementwise bar is the normwise one.  Normwise error <= RTOL * max|f| is asserted for every
+# field as well, and the CUDA path's error against the float64 oracle must stay within
 # max(X64_FLOOR, X64_FACTOR x the float32 oracle's own).
 #
 # Diagnostic fields (cloud cover, surface radiation) carry more float32 noise than the
@@ -28,8 +32,8 @@ import numpy as np
 # (conditional_diagnostics64), so that it tests the cloud and radiation arithmetic rather than
 # sqrt's magnification of precipitation rounding.  Their elementwise figures are reported.
 RTOL = 1e-5
-ELEM_FLOOR = {"u_wind": 1e-3, "v_wind": 1e-3, "precnv": 1.0, "precls": 1e-3,
-              "temperature": 1.0, "specific_humidity": 1.0}
+ELEM_FLOOR = {"u_wind": 1e-3, "v_wind": 1e-3, "precnv": 0.5, "precls": 1e-3,
+              "temperature": 1.0, "specific_humidity": 0.5}
 REPORT_FLOOR = 1e-3  # the floor at which elementwise counts are also reported for every field
 FLIP_ULPS = 64
 NOISE_FACTOR = 2.0
