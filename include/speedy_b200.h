@@ -67,12 +67,18 @@ enum spd_flags {
    * integer levels are written as usual.  This is DiagnosticsCollector's running average
    * (jcm/model.py:46-64: data[i] += new / steps) without a pass over PhysicsData per physics
    * step: zero the buffers, make the steps' calls, scale by 1/steps once. */
-  SPD_LOW_LEVEL_WINDS = 1u << 7
+  SPD_LOW_LEVEL_WINDS = 1u << 7,
   /* Forward only: spd_inputs_t.u_wind / v_wind and spd_outputs_t.u_wind / v_wind are single
    * [ix][il] planes holding the lowest level.  The physics reads the winds at the lowest level
    * only (surface_flux.py:57-58) and its wind tendencies are zero above it (surface_flux.py
    * :294-295), so a caller that keeps those zeros itself moves 2 (kx - 1) fewer planes each
    * way (the reference returns dense [kx][ix][il] planes; the default writes them). */
+  SPD_NO_SPECULATION = 1u << 8
+  /* Forward only: form the level set of cloud tops before the columns that need it (a light
+   * launch over every column, then the fused launch) instead of predicting it from the
+   * previous call.  Implied by SPD_ACCUMULATE_DIAGNOSTICS, whose added diagnostics a redone
+   * column would add twice.  A caller whose every call is a new instance (a fresh plan per
+   * batch) sets it: there is no previous call to predict from. */
 };
 
 /* One grid instance: shape, switches and DateData (jcm/date.py:9-14). */

@@ -22,6 +22,7 @@ SPD_FUSE_VERIFY = 1 << 4
 SPD_OROGRAPHIC = 1 << 5
 SPD_ACCUMULATE_DIAGNOSTICS = 1 << 6
 SPD_LOW_LEVEL_WINDS = 1 << 7
+SPD_NO_SPECULATION = 1 << 8
 
 
 class Desc(C.Structure):

@@ -37,14 +37,16 @@ class Ensemble:
 
     def __init__(self, members: List[Member], date, parameters: Optional[Parameters] = None,
                  fuse_verify=False, time_step=None, q_tend_scale=1.0,
-                 orographic_correction=False, low_level_winds=False):
+                 orographic_correction=False, low_level_winds=False, speculate=True):
         lib = _lib.load()
         self.low_level_winds = low_level_winds
+        self.speculate = speculate
         self.members = members
         self.date = date
         self.phys = SpeedyPhysics(parameters, fuse_verify=fuse_verify, time_step=time_step,
                                   q_tend_scale=q_tend_scale, diagnostics=False,
-                                  orographic_correction=orographic_correction)
+                                  orographic_correction=orographic_correction,
+                                  speculate=speculate)
         dev = members[0].state.temperature.device
         self.device = dev
         _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())
@@ -118,8 +120,11 @@ class Ensemble:
 
     def forward(self, grid_blocks=None, marker=None):
         """Runs every member.  ``marker`` (a torch.cuda.Event) is recorded between the two
-        launches (the first and second halves of the column physics), for timing them
-        separately."""
+        launches, for timing them separately: after the fused launch (before the fixup) when
+        ``speculate``, after the level-set launch (before the fused one) otherwise.  With
+        ``speculate`` each member's cloud-top level set is predicted from the previous call
+        (the plan keeps it), checked on the device, and only members whose prediction missed
+        are computed again (``redone()`` counts them)."""
         lib = _lib.load()
         gb = self.grid_blocks if grid_blocks is None else grid_blocks
         stream = torch.cuda.current_stream(self.device).cuda_stream
@@ -129,6 +134,13 @@ class Ensemble:
                                          int(gb), C.c_void_p(stream), ev)
         _lib.check(rc, "spd_ensemble_fwd")
         return [m.out for m in self.members]
+
+    def redone(self):
+        """Members the forward has computed a second time because their predicted level set
+        missed, over every call on this plan (the first call misses for every member)."""
+        nw = (self.info.nmembers + 3) & ~3
+        off = int(self.info.levelset_offset) + 16 + 12 * nw
+        return int(self.plan[off:off + 4].view(torch.int32).item())
 
     def autotune(self, candidates=None, reps=5):
         """Picks the launch shape by timing the candidates (CUDA events): persistent grids of

@@ -1,16 +1,18 @@
 // speedy_api.cu -- C-ABI entry points of the plain per-instance drop-in.
 //
-// spd_fwd runs two launches on the caller's stream, together the fused physics of every
-// column (speedy_physics.py:88-127); both are the batched kernels of speedy_ensemble.cu, run
-// over a one-member plan passed by value:
-//   1. ensemble_moist: humidity, convection, large-scale condensation and clouds.  Every column
-//      forms its cloud-top level clip(icltop, 0, kx-1) and the instance ORs them into one
-//      32-bit level set S (the cross-column dependency of shortwave_radiation.py:62-68); the
-//      same launch writes the per-latitude solar table and stages the column's partial
-//      tendencies, qsat and cloud scalars in the output planes.
-//   2. ensemble_columns: radiation, surface fluxes and vertical diffusion, reading S and the
-//      stage, then verify_tendencies and every output.
-// One thread owns one column (speedy_kernels.cuh, speedy_column_smem.cuh).
+// spd_fwd runs the physics of every column (speedy_physics.py:88-127) on the caller's stream
+// with the batched kernels of speedy_ensemble.cu over a one-member plan passed by value.  The
+// one cross-column dependency is the instance's cloud-top level set S (an OR over the columns'
+// clip(icltop, 0, kx-1), shortwave_radiation.py:62-68), which the shortwave of every column
+// reads.  By default the call predicts S from the previous call on the same scratch:
+//   1. ensemble_fused: every column whole, in one pass, its shortwave using the predicted S
+//      while the columns OR their own cloud tops into the true S; the last block to finish
+//      compares the two and keeps the true one as the next prediction;
+//   2. ensemble_fixup: returns at once when the prediction held, else computes every column
+//      again with the true S.
+// With SPD_NO_SPECULATION (or SPD_ACCUMULATE_DIAGNOSTICS) a light launch forms S first
+// (ensemble_levelset) and ensemble_fused reads it.  One thread owns one column
+// (speedy_kernels.cuh, speedy_column_smem.cuh).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,7 +20,7 @@
 
 namespace spd {
 
-constexpr size_t kHeaderBytes = 256;  // S word, status word, padding
+constexpr size_t kHeaderBytes = 256;  // launch words and level-set state, padding
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
@@ -112,9 +114,11 @@ Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_
 
 // The forward of one instance: the batched kernels over an implicit one-member plan passed
 // by value (tile t = columns t*kNT ..), one block per tile.  The plain and the batched path
-// therefore run the same code and agree bitwise.
+// therefore run the same code and agree bitwise.  `header` is the instance's 256-byte scratch
+// header: words 0-1 the launch words, 4-6 the level-set state T, R, P (stride 1), 7 the
+// cumulative count of redone calls; words 0-5 are cleared by every call, P and the count kept.
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
-                 uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker) {
+                 uint32_t* header, cudaStream_t st, cudaEvent_t marker) {
   if (kx != 7 && kx != 8 && kx != 16) return SPD_ERR_KX;
   ClassArgs A;
   A.cls[0] = CD;
@@ -125,10 +129,16 @@ int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_ou
   T.single.il = CD.K.il;
   T.single.kx = kx;
   T.single.cls = 0;
-  T.single.S = S;
-  T.single.table = table;
+  T.single.S = header + 4;
+  T.single.ls_stride = 1;
+  T.nmembers = 1;
+  T.launch = header;
+  T.redone = header + 7;
+  const bool speculate =
+      (CD.K.flags & (SPD_ACCUMULATE_DIAGNOSTICS | SPD_NO_SPECULATION)) == 0;
   const int ntiles = (CD.K.C + kNT - 1) / kNT;
-  return launch_forward(A, T, ntiles, kx, SPD_GRID_PER_TILE, st, marker);
+  return launch_forward(A, T, ntiles, kx, SPD_GRID_PER_TILE, speculate, 6 * sizeof(uint32_t),
+                        st, marker);
 }
 
 int preload_ensemble();
@@ -149,8 +159,7 @@ int spd_preload(void) {
 
 size_t spd_fwd_scratch_bytes(const spd_desc_t* desc) {
   if (!desc || desc->il <= 0) return 0;
-  const size_t table = (size_t)desc->il * sizeof(spd::ZonalRow);
-  return spd::kHeaderBytes + ((table + 255) / 256) * 256;
+  return spd::kHeaderBytes;
 }
 
 int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
@@ -172,11 +181,7 @@ int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_p
   spd::ConstsD CD;
   CD.K = spd::make_consts(desc, vgrid, params);
   CD.D = spd::derive_constants(desc, vgrid, params);
-  uint32_t* S = static_cast<uint32_t*>(scratch);
-  spd::ZonalRow* table =
-      reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + spd::kHeaderBytes);
-  if (cudaMemsetAsync(S, 0, spd::kHeaderBytes, st) != cudaSuccess) return SPD_ERR_CUDA;
-  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st,
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, static_cast<uint32_t*>(scratch), st,
                            static_cast<cudaEvent_t>(event));
 }
 

@@ -37,6 +37,11 @@ struct Derived {
   float tcorv[SPD_MAX_KX];    // orographic temperature profile        (orographic_correction.py:18-55)
   float qcorv[SPD_MAX_KX];    // orographic humidity profile           (orographic_correction.py:58-93)
   float gamlat, pexp;         // orographic_correction.py:110, :151
+  // date-only parts of the per-latitude solar row (get_zonal_average_fields,
+  // shortwave_radiation.py:220-296; solar, :406-452); the kernels finish each column's row
+  // from its latitude's sia and coa
+  float sol_tdecl, sol_sdecl, sol_cdecl, sol_scale;  // tan/sin/cos(decl), csolp * fdis
+  float coz1, cos_rzen, sin_rzen;
 };
 
 // Host evaluation (plain IEEE float32 arithmetic, no contraction on the host target).
@@ -111,6 +116,31 @@ inline Derived derive_constants(const spd_desc_t* d, const spd_vgrid_t* vg,
     }
     D.gamlat = (float)(gamma / (1000.0 * grav));
     D.pexp = (float)(1000.0 * grav / (rgas * gamma));
+  }
+  {  // solar (shortwave_radiation.py:406-452), csol = 4 solc, the parts without latitude
+    const float tyear = d->tyear;
+    const float pigr = 2.0f * asinf(1.0f);
+    const float alpha = 2.0f * pigr * tyear;
+    const float ca1 = cosf(alpha), sa1 = sinf(alpha);
+    const float ca2 = ca1 * ca1 - sa1 * sa1;
+    const float sa2 = 2.0f * sa1 * ca1;
+    const float ca3 = ca1 * ca2 - sa1 * sa2;
+    const float sa3 = sa1 * ca2 + sa2 * ca1;
+    const float decl = 0.006918f - 0.399912f * ca1 + 0.070257f * sa1 - 0.006758f * ca2 +
+                       0.000907f * sa2 - 0.002697f * ca3 + 0.001480f * sa3;
+    const float fdis =
+        1.000110f + 0.034221f * ca1 + 0.001280f * sa1 + 0.000719f * ca2 + 0.000077f * sa2;
+    D.sol_cdecl = cosf(decl);
+    D.sol_sdecl = sinf(decl);
+    D.sol_tdecl = D.sol_sdecl / D.sol_cdecl;
+    D.sol_scale = (1368.0f / pigr) * fdis;
+    // get_zonal_average_fields (shortwave_radiation.py:242-262)
+    const float asin1 = asinf(1.0f);
+    const float a2 = 4.0f * asin1 * (tyear + (float)(10.0 / 365.0));
+    D.coz1 = fmaxf(0.0f, cosf(a2 - 0.0f));
+    const float rzen = -cosf(a2) * 23.45f * asin1 / 90.0f;
+    D.cos_rzen = cosf(rzen);
+    D.sin_rzen = sinf(rzen);
   }
   return D;
 }

@@ -52,8 +52,8 @@ __device__ __forceinline__ void prefetch_ahead(const TileSource& T, int t, int s
   if (mn.C - col0n >= kNT) prefetch(mn, col0n);
 }
 
-// Launch 1: every member's per-latitude solar table and cloud-top level set S (an OR over its
-// columns' clipped cloud tops, formed by the first half's top-only form).
+// Level-set launch (when the forward does not speculate): every member's cloud-top level set
+// T, an OR over its columns' clipped cloud tops, formed by the first half's top-only form.
 __global__ void __launch_bounds__(kNT, 5) ensemble_levelset(const __grid_constant__ ClassArgs A,
                                                             const __grid_constant__ TileSource T,
                                                             int ntiles, int pf_stride) {
@@ -66,7 +66,6 @@ __global__ void __launch_bounds__(kNT, 5) ensemble_levelset(const __grid_constan
     const int c = col0 + threadIdx.x;
     const ConstsD& CD = A.cls[m.cls];
     prefetch_ahead(T, t, pf_stride, ntiles, prefetch_levelset_tile);
-    if (c < m.il) m.table[c] = zonal_row(CD.K.tyear, __ldg(m.in.sia + c), __ldg(m.in.coa + c));
     uint32_t bit = 0;
     if (c < m.C) {
       switch (m.kx) {  // uniform per block
@@ -75,25 +74,100 @@ __global__ void __launch_bounds__(kNT, 5) ensemble_levelset(const __grid_constan
         default: bit = levelset_bit<7>(CD, m.in, c, m.C); break;
       }
     }
-    or_level_set(bit, m.S);
+    or_level_set(bit, m.S + LS_T * m.ls_stride);
   }
 }
 
-// Launch 2: every column whole (fused_process), reading its member's S and solar table.
+template <int KX>
+__device__ __forceinline__ uint32_t fused_column(const ConstsD& CD, float* sm,
+                                                 const MemberDev& m, const uint32_t* S, int c) {
+  return fused_process<KX>(CD, sm, m.in, m.out, S, c, m.C, m.il);
+}
+
+// The end of a fused launch, in its last block to finish: every member's P becomes the level
+// set its columns formed (T); when speculating, R marks the members whose prediction P missed,
+// the launch word ANY says whether any did, and the cumulative count grows by their number.
+__device__ __forceinline__ void finish_fused(const TileSource& T, bool speculate) {
+  __shared__ uint32_t last, redo_block;
+  __syncthreads();  // this block's level-set ORs are issued (or_level_set ends with a barrier)
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(T.launch + LW_DONE, 1u) == gridDim.x - 1;
+    redo_block = 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int nm = T.members ? T.nmembers : 1;
+  uint32_t redo = 0;
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) {
+    const MemberDev& m = T.members ? T.members[i] : T.single;
+    volatile uint32_t* S = m.S;
+    const uint32_t t = S[LS_T * m.ls_stride];
+    if (speculate) {
+      const uint32_t r = t != S[LS_P * m.ls_stride] ? 1u : 0u;
+      S[LS_R * m.ls_stride] = r;
+      redo += r;
+    }
+    S[LS_P * m.ls_stride] = t;
+  }
+  if (redo) atomicAdd(&redo_block, redo);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T.launch[LW_ANY] = redo_block ? 1u : 0u;
+    if (redo_block) atomicAdd(T.redone, redo_block);
+  }
+}
+
+// Fused launch: every column whole (fused_process).  speculate = 1: the shortwave uses each
+// member's predicted level set P while the columns OR their own cloud tops into T; else T is
+// complete (the level-set launch formed it) and the columns read it.
 __global__ void __launch_bounds__(kNT, 4) ensemble_fused(const __grid_constant__ ClassArgs A,
                                                          const __grid_constant__ TileSource T,
-                                                         int ntiles) {
+                                                         int ntiles, int speculate) {
   extern __shared__ float sm[];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     int col0;
     const MemberDev m = tile_member(T, t, col0);
     const int c = col0 + threadIdx.x;
+    const uint32_t* S = m.S + (speculate ? LS_P : LS_T) * m.ls_stride;
+    uint32_t bit = 0;
     if (c < m.C) {
       const ConstsD& CD = A.cls[m.cls];
       switch (m.kx) {
-        case 16: fused_process<16>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
-        case 8: fused_process<8>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
-        default: fused_process<7>(CD, sm, m.in, m.out, m.S, m.table, c, m.C, m.il); break;
+        case 16: bit = fused_column<16>(CD, sm, m, S, c); break;
+        case 8: bit = fused_column<8>(CD, sm, m, S, c); break;
+        default: bit = fused_column<7>(CD, sm, m, S, c); break;
+      }
+    }
+    if (speculate) or_level_set(bit, m.S + LS_T * m.ls_stride);
+  }
+  // the fixup launch may start as this one's blocks retire; it waits for completion
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  finish_fused(T, speculate != 0);
+}
+
+// Fixup launch after a speculating fused launch: the members whose prediction missed (R set)
+// are computed again with their true level set (P, now equal to T).  In the common case no
+// member missed and every block returns after reading one word.
+__global__ void __launch_bounds__(kNT, 4) ensemble_fixup(const __grid_constant__ ClassArgs A,
+                                                         const __grid_constant__ TileSource T,
+                                                         int ntiles) {
+  extern __shared__ float sm[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (*reinterpret_cast<volatile uint32_t*>(T.launch + LW_ANY) == 0u) return;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int col0;
+    const MemberDev m = tile_member(T, t, col0);
+    if (*reinterpret_cast<volatile uint32_t*>(m.S + LS_R * m.ls_stride) == 0u) continue;
+    const int c = col0 + threadIdx.x;
+    const uint32_t* S = m.S + LS_P * m.ls_stride;
+    if (c < m.C) {
+      const ConstsD& CD = A.cls[m.cls];
+      switch (m.kx) {
+        case 16: fused_column<16>(CD, sm, m, S, c); break;
+        case 8: fused_column<8>(CD, sm, m, S, c); break;
+        default: fused_column<7>(CD, sm, m, S, c); break;
       }
     }
   }
@@ -121,6 +195,8 @@ int residency(Residency& R) {
     Residency r;
     if (cudaFuncSetAttribute(ensemble_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem_bytes<16>()) != cudaSuccess ||
+        cudaFuncSetAttribute(ensemble_fixup, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem_bytes<16>()) != cudaSuccess ||
         cudaDeviceGetAttribute(&r.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.lvl, ensemble_levelset, kNT, 0) !=
             cudaSuccess)
@@ -139,8 +215,29 @@ int residency(Residency& R) {
 }
 }  // namespace
 
+// Launches kernel<<<grid, kNT, smem, st>>>(args...) as a programmatic dependent launch: its
+// blocks may start as the previous launch's blocks retire (they wait on the device,
+// griddepcontrol.wait, before reading what that launch writes).
+template <class... KArgs, class... Args>
+static int launch_dependent(void (*kernel)(KArgs...), int grid, size_t smem, cudaStream_t st,
+                            Args... args) {
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kNT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, kernel, args...) != cudaSuccess) return SPD_ERR_CUDA;
+  return SPD_OK;
+}
+
 int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_layout,
-                   int grid_blocks, cudaStream_t st, cudaEvent_t marker) {
+                   int grid_blocks, bool speculate, size_t clear_bytes, cudaStream_t st,
+                   cudaEvent_t marker) {
   Residency R;
   const int rc = residency(R);
   if (rc != SPD_OK) return rc;
@@ -156,25 +253,30 @@ int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_l
     grid_cols = std::min(grid_blocks > 0 ? grid_blocks : res_cols, ntiles);
     pf_lvl = grid_lvl;
   }
-  ensemble_levelset<<<grid_lvl, kNT, 0, st>>>(A, T, ntiles, pf_lvl);
-  if (marker) {  // timing hook: the two launches apart, in plain stream order
-    if (cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
-    ensemble_fused<<<grid_cols, kNT, arena_bytes(kx_layout), st>>>(A, T, ntiles);
-    return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
+  const size_t arena = arena_bytes(kx_layout);
+  // the launch words and every member's T and R start at zero; P is kept from the last call
+  if (cudaMemsetAsync(T.launch, 0, clear_bytes, st) != cudaSuccess) return SPD_ERR_CUDA;
+  int r;
+  if (speculate) {
+    ensemble_fused<<<grid_cols, kNT, arena, st>>>(A, T, ntiles, 1);
+    if (marker) {  // timing hook: the fused launch apart, then the fixup in plain stream order
+      if (cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
+      ensemble_fixup<<<grid_cols, kNT, arena, st>>>(A, T, ntiles);
+      r = SPD_OK;
+    } else {
+      r = launch_dependent(ensemble_fixup, grid_cols, arena, st, A, T, ntiles);
+    }
+  } else {
+    ensemble_levelset<<<grid_lvl, kNT, 0, st>>>(A, T, ntiles, pf_lvl);
+    if (marker) {  // timing hook: the two launches apart, in plain stream order
+      if (cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
+      ensemble_fused<<<grid_cols, kNT, arena, st>>>(A, T, ntiles, 0);
+      r = SPD_OK;
+    } else {
+      r = launch_dependent(ensemble_fused, grid_cols, arena, st, A, T, ntiles, 0);
+    }
   }
-  // programmatic dependent launch: the second launch's blocks take SMs as the first launch's
-  // blocks retire and load their inputs, then wait (griddepcontrol.wait) for its completion
-  cudaLaunchAttribute attr;
-  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr.val.programmaticStreamSerializationAllowed = 1;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid_cols);
-  cfg.blockDim = dim3(kNT);
-  cfg.dynamicSmemBytes = arena_bytes(kx_layout);
-  cfg.stream = st;
-  cfg.attrs = &attr;
-  cfg.numAttrs = 1;
-  if (cudaLaunchKernelEx(&cfg, ensemble_fused, A, T, ntiles) != cudaSuccess) return SPD_ERR_CUDA;
+  if (r != SPD_OK) return r;
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
@@ -182,6 +284,7 @@ int preload_ensemble() {
   cudaFuncAttributes a;
   bool ok = cudaFuncGetAttributes(&a, ensemble_levelset) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, ensemble_fused) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_fixup) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 
@@ -225,11 +328,15 @@ int spd_ensemble_plan(const spd_class_t* classes, int nclasses, const spd_member
     md[i].kx = classes[m.cls].desc.kx;
     md[i].cls = m.cls;
   }
-  const int t = plan_tiles(md, nmembers, L, dbase, reinterpret_cast<Tile*>(h + L.tiles));
+  for (int i = 0; i < nmembers; ++i) {
+    md[i].S = levelset_T(L, dbase) + i;
+    md[i].ls_stride = L.nw;
+  }
+  const int t = plan_tile_list(md, nmembers, reinterpret_cast<Tile*>(h + L.tiles));
   info->nmembers = nmembers;
   info->ntiles = t;
   info->levelset_offset = L.levelset;
-  info->levelset_bytes = align256((size_t)nmembers * sizeof(uint32_t));
+  info->levelset_bytes = levelset_region_bytes(L.nw);
   info->plan_bytes = L.total;
   return SPD_OK;
 }
@@ -257,14 +364,20 @@ int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan
   if (kx_layout != 7 && kx_layout != 8 && kx_layout != 16) return SPD_ERR_KX;
   char* base = static_cast<char*>(plan_device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  bool speculate = true;
+  for (int i = 0; i < nclasses; ++i)
+    if (classes[i].desc.flags & (SPD_ACCUMULATE_DIAGNOSTICS | SPD_NO_SPECULATION))
+      speculate = false;
+  const int nw = (info->nmembers + 3) & ~3;
   TileSource T{};
   T.members = reinterpret_cast<const MemberDev*>(base + 256);
   T.tiles = reinterpret_cast<const Tile*>(
       base + 256 + align256((size_t)info->nmembers * sizeof(MemberDev)));
-  if (cudaMemsetAsync(base + info->levelset_offset, 0, info->levelset_bytes, st) != cudaSuccess)
-    return SPD_ERR_CUDA;
-  return launch_forward(A, T, info->ntiles, kx_layout, grid_blocks, st,
-                        static_cast<cudaEvent_t>(event));
+  T.nmembers = info->nmembers;
+  T.launch = reinterpret_cast<uint32_t*>(base + info->levelset_offset);
+  T.redone = T.launch + (16 + 12 * (size_t)nw) / sizeof(uint32_t);
+  return launch_forward(A, T, info->ntiles, kx_layout, grid_blocks, speculate,
+                        16 + 8 * (size_t)nw, st, static_cast<cudaEvent_t>(event));
 }
 
 }  // extern "C"

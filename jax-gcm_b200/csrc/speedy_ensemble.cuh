@@ -11,12 +11,20 @@
 
 namespace spd {
 
+// Level-set state of a member in the forward: S points at its accumulator T of the true level
+// set; R (S[ls_stride]) is its redo flag and P (S[2 ls_stride]) the level set its last forward
+// used, which the next forward predicts.
+enum { LS_T = 0, LS_R = 1, LS_P = 2 };
+// Words of one forward launch (TileSource::launch): the count of blocks done, whether any member
+// must be redone, and (cumulative, in the region's last 16 bytes) the members redone so far.
+enum { LW_DONE = 0, LW_ANY = 1 };
+
 struct MemberDev {
   spd_inputs_t in;
   spd_outputs_t out;
   int C, il, kx, cls;
   uint32_t* S;
-  ZonalRow* table;
+  int ls_stride, reserved;
 };
 
 struct ClassArgs {
@@ -34,6 +42,9 @@ struct TileSource {
   const MemberDev* members;
   const Tile* tiles;
   MemberDev single;
+  int nmembers;
+  uint32_t* launch;   // the launch words
+  uint32_t* redone;   // cumulative count of members redone
 };
 
 // The member of tile t, copied: the kernels read its field pointers from the copy, which no
@@ -60,12 +71,16 @@ __device__ __forceinline__ void prefetch_tile_rows(int nrows, RowFn row) {
   }
 }
 
-// Both launches of the forward (speedy_ensemble.cu) over the ntiles tiles.  grid_blocks: 0 =
-// persistent grids of SMs x resident blocks; > 0 = the second launch's persistent grid;
+// The forward (speedy_ensemble.cu) over the ntiles tiles, after clearing the launch words and
+// every member's T and R (clear_bytes from T.launch).  speculate: the fused launch uses each
+// member's predicted level set P and a fixup launch redoes the members whose prediction missed;
+// otherwise a level-set launch forms every T before the fused launch reads it.  grid_blocks:
+// 0 = persistent grids of SMs x resident blocks; > 0 = the fused launch's persistent grid;
 // SPD_GRID_PER_TILE = one block per tile.  kx_layout is the largest level count among the
-// tiles (it sizes the second launch's shared-memory arena).
+// tiles (it sizes the fused launch's shared-memory arena).
 int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_layout,
-                   int grid_blocks, cudaStream_t st, cudaEvent_t marker);
+                   int grid_blocks, bool speculate, size_t clear_bytes, cudaStream_t st,
+                   cudaEvent_t marker);
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -93,11 +108,16 @@ __device__ __forceinline__ void prepass_tiles(const ClassArgs& A, const M* __res
   }
 }
 
-// Device plan layout: header, member records, tile list, level-set words, solar tables.
+// Device plan layout: header, member records, tile list, level-set region, solar tables.  The
+// level-set region: 16 bytes of launch words, then nw words each of every member's T, R and P
+// (nw = member count rounded up to 4), then 16 bytes whose first word counts the members the
+// forward redid (its prediction missed).
 struct PlanLayout {
   size_t members, tiles, levelset, tables, total;
-  int ntiles;
+  int ntiles, nw;
 };
+
+inline size_t levelset_region_bytes(int nw) { return 16 + 12 * (size_t)nw + 16; }
 
 // HM: host member description with ix and il.
 template <class HM>
@@ -113,10 +133,29 @@ inline PlanLayout plan_layout(const HM* members, int n, size_t record_bytes) {
   L.ntiles = ntiles;
   L.members = 256;
   L.tiles = L.members + align256((size_t)n * record_bytes);
+  L.nw = (n + 3) & ~3;
   L.levelset = L.tiles + align256((size_t)ntiles * sizeof(Tile));
-  L.tables = L.levelset + align256((size_t)n * sizeof(uint32_t));
+  L.tables = L.levelset + align256(levelset_region_bytes(L.nw));
   L.total = L.tables + tab;
   return L;
+}
+
+// The members' T words (device address) in a plan at dbase.
+inline uint32_t* levelset_T(const PlanLayout& L, char* dbase) {
+  return reinterpret_cast<uint32_t*>(dbase + L.levelset + 16);
+}
+
+// The tile list: tiles of 16-level members first, then fewer levels (heavier work first).
+// Returns the tile count.  DM: device member record with C and kx.
+template <class DM>
+inline int plan_tile_list(const DM* md, int n, Tile* tl) {
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return md[a].kx > md[b].kx; });
+  int t = 0;
+  for (int i : order)
+    for (int c0 = 0; c0 < md[i].C; c0 += kNT) tl[t++] = Tile{i, c0};
+  return t;
 }
 
 // Fills each record's level-set and table pointers (device addresses) and the tile list:
@@ -126,17 +165,11 @@ template <class DM>
 inline int plan_tiles(DM* md, int n, const PlanLayout& L, char* dbase, Tile* tl) {
   size_t tab = L.tables;
   for (int i = 0; i < n; ++i) {
-    md[i].S = reinterpret_cast<uint32_t*>(dbase + L.levelset) + i;
+    md[i].S = levelset_T(L, dbase) + i;
     md[i].table = reinterpret_cast<ZonalRow*>(dbase + tab);
     tab += align256((size_t)md[i].il * sizeof(ZonalRow));
   }
-  std::vector<int> order(n);
-  for (int i = 0; i < n; ++i) order[i] = i;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return md[a].kx > md[b].kx; });
-  int t = 0;
-  for (int i : order)
-    for (int c0 = 0; c0 < md[i].C; c0 += kNT) tl[t++] = Tile{i, c0};
-  return t;
+  return plan_tile_list(md, n, tl);
 }
 
 }  // namespace spd

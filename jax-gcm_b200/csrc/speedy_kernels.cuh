@@ -173,19 +173,42 @@ __device__ __forceinline__ void column_outputs(const ConstsD& CD, float* sm,
   if (out.icltop) out.icltop[c] = o.icltop;
 }
 
+// The solar row of a column at latitude (sia, coa), finished from the launch's date-only parts
+// (Derived): get_zonal_average_fields (shortwave_radiation.py:220-296) with solar (:406-452).
+__device__ __forceinline__ ZonalRow zonal_row_of(const Derived& D, float sia, float coa) {
+  // clip bounds -1+1e-9 and 1-1e-9 round to -1 and 1 in float32
+  const float ch0 = fminf(fmaxf(-D.sol_tdecl * sia / coa, (float)(-1.0 + 1e-9)),
+                          (float)(1.0 - 1e-9));
+  const float h0 = acosf(ch0);
+  const float sh0 = sinf(h0);
+  const float fsol = D.sol_scale * (h0 * sia * D.sol_sdecl + sh0 * coa * D.sol_cdecl);
+  const float flat2 = 1.5f * (sia * sia) - 0.5f;
+  const float ozone = (float)(0.4 * 0.02) * (1.0f + D.coz1 * sia + 1.8f * flat2);
+  const float base = 1.0f - (coa * D.cos_rzen + sia * D.sin_rzen);
+  const float zenit = 1.0f + base * base;
+  ZonalRow r;
+  r.fsol = fsol;
+  r.ozupp = fsol * 0.01f * zenit;
+  r.ozone = fsol * ozone * zenit;
+  r.zenit = zenit;
+  r.stratz = fmaxf(6.0f - fsol, 0.0f);
+  r.sqrt_coa = sqrtf(coa);
+  r.pad0 = r.pad1 = 0.0f;
+  return r;
+}
+
 // The whole column c in one pass: the first half (humidity through clouds) with its level
 // arrays in registers, its results and the state moved into the block's shared-memory arena,
 // then the second half (radiation, surface fluxes, vertical diffusion) and the outputs.  The
-// instance's cloud-top level set *S and its per-latitude solar table come from the level-set
-// launch before this one; they are read only after the first half, behind griddepcontrol.wait
-// (when this launch overlaps that one's tail, it waits there for that launch's completion;
-// otherwise it returns at once).
+// shortwave uses the level set *S (the instance's, or its prediction); S is read only after the
+// first half, behind griddepcontrol.wait (when this launch overlaps the tail of a launch it
+// depends on, it waits there for that launch's completion; otherwise it returns at once).
+// Returns the column's own cloud-top level bit, 1 << clip(icltop, 0, kx-1).
 template <int KX>
-__device__ __forceinline__ void fused_process(const ConstsD& CD, float* sm,
-                                              const spd_inputs_t& in, const spd_outputs_t& out,
-                                              const uint32_t* S,
-                                              const ZonalRow* __restrict__ table, int c, int C,
-                                              int il) {
+__device__ __forceinline__ uint32_t fused_process(const ConstsD& CD, float* sm,
+                                                  const spd_inputs_t& in,
+                                                  const spd_outputs_t& out, const uint32_t* S,
+                                                  int c, int C, int il) {
   const Consts& K = CD.K;
   const bool verify = (K.flags & SPD_FUSE_VERIFY) != 0;
   const bool low = (K.flags & SPD_LOW_LEVEL_WINDS) != 0;
@@ -234,11 +257,13 @@ __device__ __forceinline__ void fused_process(const ConstsD& CD, float* sm,
   s.alb0 = __ldg(in.alb0 + c);
   s.orog = __ldg(in.orog + c);
   s.phis0 = __ldg(in.phis0 + c);
+  const int j = c % il;
+  const ZonalRow z = zonal_row_of(CD.D, __ldg(in.sia + j), __ldg(in.coa + j));
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const uint32_t Sw = *S;
-  const ZonalRow z = table[c % il];
+  const uint32_t Sw = *reinterpret_cast<const volatile uint32_t*>(S);
   column_second<KX>(CD, sm, s, z, Sw, o);
   column_outputs<KX>(CD, sm, in, out, s, o, neg, c, C);
+  return 1u << min(max(o.icltop, 0), KX - 1);
 }
 
 }  // namespace spd

@@ -3,10 +3,12 @@
 // Some callers have no way to obtain device scratch: a foreign-function bridge (cgo, JNI, a
 // ctypes stub) that only forwards the state, forcing and tendency buffers handed to it, or a
 // process whose device memory is owned entirely by another runtime's pooling allocator.  This
-// entry point needs no scratch argument and performs no allocation: its scratch (the
-// instance's cloud-top level set word, a status word and the per-latitude solar table) lives
-// in the fixed file-scope device array below, sized for at most SPD_NOALLOC_MAX_IL latitudes.
-// Every GPU that loads the library keeps that array (65,792 bytes) until the process exits.
+// entry point needs no scratch argument and performs no allocation: its scratch lives in the
+// fixed file-scope device array below.  The call's launch words and the instance's level-set
+// state take its first 256 bytes; the rest holds up to SPD_NOALLOC_MAX_IL rows of a
+// per-latitude table (the size limit of the entry point; the present kernels form each
+// column's solar row themselves and leave it unused).  Every GPU that loads the library keeps
+// that array (65,792 bytes) until the process exits.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,12 +20,12 @@ int check_forward_instance(const spd_desc_t* d, const spd_inputs_t* in,
                            const spd_outputs_t* out);
 Consts make_consts(const spd_desc_t* d, const spd_vgrid_t* vg, const spd_params_t* p);
 int dispatch_fwd(const ConstsD& CD, int kx, const spd_inputs_t& in, const spd_outputs_t& out,
-                 uint32_t* S, ZonalRow* table, cudaStream_t st, cudaEvent_t marker);
+                 uint32_t* header, cudaStream_t st, cudaEvent_t marker);
 }  // namespace spd
 
 namespace {
 
-constexpr size_t kNoallocHeader = 256;  // level-set word, status word, padding
+constexpr size_t kNoallocHeader = 256;  // launch words, level-set state, padding
 constexpr size_t kNoallocBytes = kNoallocHeader + (size_t)SPD_NOALLOC_MAX_IL * sizeof(spd::ZonalRow);
 
 // The shared scratch.  In host code this name is only a host-side stand-in for the symbol;
@@ -68,11 +70,10 @@ extern "C" int spd_fwd_noalloc(const spd_desc_t* desc, const spd_vgrid_t* vgrid,
   spd::ConstsD CD;
   CD.K = spd::make_consts(desc, vgrid, params);
   CD.D = spd::derive_constants(desc, vgrid, params);
-  uint32_t* S = static_cast<uint32_t*>(scratch);
-  spd::ZonalRow* table =
-      reinterpret_cast<spd::ZonalRow*>(static_cast<char*>(scratch) + kNoallocHeader);
-  // The array keeps the previous call's contents: the level-set and status words must start
-  // at zero; the solar table is fully rewritten by the first launch.
-  if (cudaMemsetAsync(S, 0, kNoallocHeader, st) != cudaSuccess) return SPD_ERR_CUDA;
-  return spd::dispatch_fwd(CD, desc->kx, *in, *out, S, table, st, nullptr);
+  // The array keeps the previous call's contents: the call clears the words that must start
+  // at zero itself, and keeps the previous call's level set as its prediction (a prediction
+  // that misses, e.g. after another instance's call, costs a second pass, never a wrong
+  // result).
+  return spd::dispatch_fwd(CD, desc->kx, *in, *out, static_cast<uint32_t*>(scratch), st,
+                           nullptr);
 }

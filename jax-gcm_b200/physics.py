@@ -394,6 +394,11 @@ class Physics:
     def compute_tendencies(self, state, forcing, geometry, date):
         raise NotImplementedError("Physics compute_tendencies method not implemented.")
 
+    def speculating(self, accumulate=False):
+        """Whether a call predicts the level set (see the class docstring); accumulating
+        diagnostics never does (a redone column would add its diagnostics twice)."""
+        return self.speculate and not accumulate
+
     def get_empty_data(self, geometry):
         return None
 
@@ -433,11 +438,19 @@ class SpeedyPhysics(Physics):
     ``orographic_correction=True`` appends the orographic correction as the last term
     (orographic_correction.py:177-247), which the reference's term list carries commented out
     (speedy_physics.py:65,79).
+
+    ``speculate=True`` (the default) predicts the instance's cloud-top level set (the one
+    cross-column dependency, shortwave_radiation.py:62-68) from this object's previous call
+    and checks it on the device: the physics runs in one pass over the columns, and a second
+    pass follows only when the prediction missed (the first call, or after another instance's
+    call).  ``speculate=False`` forms the level set first in a light launch.  Both give the same
+    results bitwise.  Calls of one object use one scratch buffer: order them on one stream.
     """
 
     def __init__(self, parameters: Optional[Parameters] = None, checkpoint_terms=True,
                  fuse_verify=False, time_step=None, q_tend_scale=1.0, diagnostics=True,
-                 orographic_correction=False):
+                 orographic_correction=False, speculate=True):
+        self.speculate = speculate
         self.parameters = parameters or Parameters.default()
         self.fuse_verify = fuse_verify
         self.orographic_correction = orographic_correction
@@ -460,6 +473,8 @@ class SpeedyPhysics(Physics):
             if self.time_step is not None and float(self.time_step) != float(date.dt_seconds):
                 raise ValueError("orographic_correction needs time_step == date.dt_seconds")
             flags |= _lib.SPD_OROGRAPHIC
+        if not self.speculate:
+            flags |= _lib.SPD_NO_SPECULATION
         dt = date.dt_seconds if self.time_step is None else self.time_step
         return _lib.Desc(kx, ix, il, flags, float(np.float32(date.tyear)), int(date.model_year),
                          int(date.model_step), int(self.parameters.forcing.co2_year_ref),
@@ -480,8 +495,9 @@ class SpeedyPhysics(Physics):
                            accumulate: bool = False):
         """Tendencies and PhysicsData for ``state``.  ``out`` may give preallocated output
         tensors (they must not overlap the inputs); ``marker`` (a torch.cuda.Event) is recorded
-        between the two launches (the first and second halves of the column physics), for
-        timing them separately.  ``accumulate=True`` adds precnv, precls and the float
+        between the call's two launches, for timing them separately: after the fused launch
+        (before the fixup) when speculating, after the level-set launch (before the fused one)
+        otherwise (``speculating(accumulate)`` says which).  ``accumulate=True`` adds precnv, precls and the float
         diagnostics to what ``out`` holds instead of overwriting them (the running sums of
         DiagnosticsCollector, jcm/model.py:46-64; scale by 1/steps once at the end)."""
         if accumulate and out is None:

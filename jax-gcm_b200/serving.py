@@ -712,9 +712,16 @@ class CudaBackend:
         self._h0 = 0.0
 
     # -- sizes ----------------------------------------------------------------------------------
-    def _desc(self, kx, ix, il, lfluxland):
+    def _desc(self, kx, ix, il, lfluxland, forward=False):
+        """The instance descriptor.  Forward calls form the cloud-top level set before the
+        columns (SPD_NO_SPECULATION): every tendency batch is a new plan and the plain calls
+        share one scratch across members, so there is no previous call of the same instance to
+        predict it from."""
         from types import SimpleNamespace
-        return self.phys.desc(SimpleNamespace(nodal_shape=(kx, ix, il)), self.date, lfluxland)
+        d = self.phys.desc(SimpleNamespace(nodal_shape=(kx, ix, il)), self.date, lfluxland)
+        if forward:
+            d.flags |= _lib.SPD_NO_SPECULATION
+        return d
 
     def _vjp_scratch_bytes(self, kx):
         # 512 x 256 columns reach the adjoint's thread cap, hence its largest scratch
@@ -908,7 +915,7 @@ class CudaBackend:
 
     def _fwd_plain(self, dm, req, d, stream):
         h = dm.host
-        desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+        desc = self._desc(h.kx, h.ix, h.il, h.lfluxland, forward=True)
         rc = self.lib.spd_fwd(C.byref(desc), C.byref(self.vgrid(h.kx)),
                               C.byref(self.phys._pstruct), C.byref(dm.inputs),
                               C.byref(self._outputs_struct(req, d)),
@@ -947,13 +954,13 @@ class CudaBackend:
                                   C.c_void_p(stream.cuda_stream))
             _lib.check(rc, "spd_vjp")
 
-    def _classes(self, members):
+    def _classes(self, members, forward=False):
         classes, cls_of = [], {}
         for h in members:
             key = (h.kx, h.lfluxland)
             if key not in cls_of:
                 c = _lib.Class()
-                c.desc = self._desc(h.kx, h.ix, h.il, h.lfluxland)
+                c.desc = self._desc(h.kx, h.ix, h.il, h.lfluxland, forward)
                 c.vgrid = self.vgrid(h.kx)
                 c.params = self.phys._pstruct
                 cls_of[key] = len(classes)
@@ -995,7 +1002,7 @@ class CudaBackend:
 
     def _ensemble(self, reqs, devs, stream):
         pairs = [(dm, r, d) for r, dl in zip(reqs, devs) for dm, d in zip(dl, r._views)]
-        cl, cls_of = self._classes([dm.host for dm, _, _ in pairs])
+        cl, cls_of = self._classes([dm.host for dm, _, _ in pairs], forward=True)
         mem = (_lib.Member * len(pairs))()
         for i, (dm, r, d) in enumerate(pairs):
             h = dm.host

@@ -75,9 +75,15 @@ def test_struct_sizes_match_header(pkg):
 
 
 def test_scratch_bytes(pkg, lib):
-    d = pkg._lib.Desc(8, 96, 48, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
-    n = lib.spd_fwd_scratch_bytes(C.byref(d))
-    assert n >= 256 + 48 * 32 and n % 256 == 0
+    """The forward's scratch is one 256-byte header (launch words and the instance's level-set
+    state), whatever the grid; the adjoint's holds a one-member plan and grows with it."""
+    for shape in ((8, 96, 48), (16, 1280, 640)):
+        d = pkg._lib.Desc(*shape, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+        assert lib.spd_fwd_scratch_bytes(C.byref(d)) == 256
+    small = pkg._lib.Desc(8, 96, 48, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    large = pkg._lib.Desc(16, 1280, 640, 0, 0.2, 1950, 0, 1950, 1800.0, 1.0)
+    a, b = lib.spd_vjp_scratch_bytes(C.byref(small)), lib.spd_vjp_scratch_bytes(C.byref(large))
+    assert a % 256 == 0 and b > a
 
 
 def test_argument_validation_needs_no_gpu(pkg, lib):

@@ -56,7 +56,17 @@ def test_plan_layout_and_tile_order(pkg):
         covered.setdefault(int(m), []).append(int(c0))
     for i, (ix, il, _) in enumerate(shapes):
         assert covered[i] == list(range(0, ix * il, 128))
-    assert info.levelset_offset % 256 == 0 and info.levelset_bytes >= 16
+    assert info.levelset_offset % 256 == 0
+    # the level-set region: launch words, then each member's T, R and P words (the member
+    # count rounded up to 4 apart), then the count of redone members
+    nw = 4
+    assert info.levelset_bytes == 16 + 12 * nw + 16
+    head = C.sizeof(L.Inputs) + C.sizeof(L.Outputs) + 4 * 4
+    for i in range(len(shapes)):
+        rec = 256 + i * msize
+        s_ptr = int(np.frombuffer(raw, np.uint64, 1, rec + head)[0])
+        stride = int(np.frombuffer(raw, np.int32, 1, rec + head + 8)[0])
+        assert s_ptr == dev_base + info.levelset_offset + 16 + 4 * i and stride == nw
 
 
 def test_plan_rejects_bad_class(pkg):
@@ -116,7 +126,7 @@ def test_vjp_plan_layout_tiles_and_records(pkg):
         cols, il_, kx, cls_ = np.frombuffer(raw, np.int32, 4, rec + head)
         assert (cols, il_, kx, cls_) == (ix * il, il, kx_of[i], cls)
         s_ptr, table = np.frombuffer(raw, np.uint64, 2, rec + head + 16)
-        assert s_ptr == dev_base + info.levelset_offset + 4 * i
+        assert s_ptr == dev_base + info.levelset_offset + 16 + 4 * i
         tables.add(int(table))
     assert len(tables) == len(shapes) and all(t % 256 == 0 for t in tables)
     tiles_off = 256 + ((len(shapes) * msize + 255) // 256) * 256
