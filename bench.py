@@ -292,7 +292,7 @@ def run_b200(args):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                 "kernel": ("ensemble_fused" if two
-                           else "ensemble_levelset + ensemble_fused (one forward per member)"),
+                           else "ensemble_fused + ensemble_fixup (one forward per member)"),
                 "kernel_ms": round(kern_ms, 4),
                 "algorithmic_bytes_per_launch": bytes_path,
                 "bytes_per_column": "4 (9 kx + 12)",

@@ -87,9 +87,14 @@ __device__ __forceinline__ uint32_t fused_column(const ConstsD& CD, float* sm,
 // The end of a fused launch, in its last block to finish: every member's P becomes the level
 // set its columns formed (T); when speculating, R marks the members whose prediction P missed,
 // the launch word ANY says whether any did, and the cumulative count grows by their number.
-__device__ __forceinline__ void finish_fused(const TileSource& T, bool speculate) {
-  __shared__ uint32_t last, redo_block;
-  __syncthreads();  // this block's level-set ORs are issued (or_level_set ends with a barrier)
+// `words` are two words of the block's shared memory that the columns no longer use (the
+// fused launch declares no static shared memory: one more word would leave room for three
+// blocks per SM instead of four at 16 levels).
+__device__ __forceinline__ void finish_fused(const TileSource& T, bool speculate,
+                                             uint32_t* words) {
+  uint32_t& last = words[0];
+  uint32_t& redo_block = words[1];
+  __syncthreads();  // every warp of this block has issued its level-set ORs and left the arena
   if (threadIdx.x == 0) {
     __threadfence();
     last = atomicAdd(T.launch + LW_DONE, 1u) == gridDim.x - 1;
@@ -140,11 +145,11 @@ __global__ void __launch_bounds__(kNT, 4) ensemble_fused(const __grid_constant__
         default: bit = fused_column<7>(CD, sm, m, S, c); break;
       }
     }
-    if (speculate) or_level_set(bit, m.S + LS_T * m.ls_stride);
+    if (speculate) or_level_set_warp(bit, m.S + LS_T * m.ls_stride);
   }
   // the fixup launch may start as this one's blocks retire; it waits for completion
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  finish_fused(T, speculate != 0);
+  finish_fused(T, speculate != 0, reinterpret_cast<uint32_t*>(sm));
 }
 
 // Fixup launch after a speculating fused launch: the members whose prediction missed (R set)

@@ -33,6 +33,17 @@ __device__ __forceinline__ void or_level_set(uint32_t bit, uint32_t* S) {
   __syncthreads();  // warp_bits may be rewritten by the caller's next tile
 }
 
+// The fused launch's form of or_level_set: the OR of a warp's bits, added by one lane, with no
+// block barrier (the fused launch's warps run their columns at very different speeds, and a
+// barrier per tile would hold the fast ones).  Every lane of the warp must call it.
+__device__ __forceinline__ void or_level_set_warp(uint32_t bit, uint32_t* S) {
+  bit = __reduce_or_sync(0xffffffffu, bit);
+  if ((threadIdx.x & 31) == 0) {
+    const uint32_t have = *reinterpret_cast<volatile uint32_t*>(S);
+    if ((have & bit) != bit) atomicOr(S, bit);
+  }
+}
+
 // Cloud-top level bit of column c from registers (the adjoint's pre-pass; the forward takes it
 // from its first half).
 template <int KX>

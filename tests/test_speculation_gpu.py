@@ -22,11 +22,12 @@ def pkg():
 
 
 def two_instances(pkg):
-    """Two 4x2-column instances whose level sets differ (one column saturated near level 2
-    moves its cloud top)."""
+    """Two 4x2-column instances whose level sets differ: {1} (every column's cloud top at level
+    1), and {1, 4} (one column moistened fivefold in its upper five levels condenses from level
+    4 down, which moves its cloud top there)."""
     a = pkg.synthetic.config0_instance(seed=2, ix=4, il=2, lfluxland=True)
     b = pkg.synthetic.config0_instance(seed=2, ix=4, il=2, lfluxland=True)
-    b.q[2, 0, 0] = b.q[2, 0, 0] * 40.0
+    b.q[:5, 0, 0] = b.q[:5, 0, 0] * 5.0
     return a, b
 
 
