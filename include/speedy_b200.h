@@ -41,7 +41,7 @@ enum spd_status {
   SPD_ERR_KX = 3,        /* unsupported level count (supported: 7, 8, 16) */
   SPD_ERR_SCRATCH = 4,   /* scratch buffer NULL, too small or not 256-byte aligned */
   SPD_ERR_CUDA = 5,      /* a CUDA launch or runtime call failed */
-  SPD_ERR_DEVICE = 6,    /* the device reported an error status (bounded wait expired, ...) */
+  /* 6 is not used: no kernel waits on another or reports a status of its own */
   SPD_ERR_ALIGN = 7,     /* a field pointer is not 16-byte aligned */
   SPD_ERR_NOALLOC_LIMIT = 8, /* il above SPD_NOALLOC_MAX_IL for spd_fwd_noalloc */
   SPD_ERR_ALIAS = 9,         /* an output field overlaps an input field or another output */

@@ -109,7 +109,7 @@ DIFF_PARAM_NAMES = ["psmin", "trcnv", "rhil", "rhbl", "entmax", "smf", "trlsc", 
                     "drhlsc", "rhblsc", "albcl", "albcls"]
 
 STATUS = {0: "ok", 1: "null pointer", 2: "bad shape", 3: "unsupported kx", 4: "bad scratch",
-          5: "CUDA error", 6: "device error status", 7: "misaligned pointer",
+          5: "CUDA error", 7: "misaligned pointer",
           8: "il above the no-allocation entry point's limit",
           9: "an output field overlaps an input or another output",
           10: "the stream belongs to another device than the current one"}

@@ -193,7 +193,6 @@ const char* spd_status_string(int status) {
     case SPD_ERR_KX: return "unsupported level count (supported: 7, 8, 16)";
     case SPD_ERR_SCRATCH: return "scratch buffer NULL, too small or not 256-byte aligned";
     case SPD_ERR_CUDA: return "CUDA launch or runtime call failed";
-    case SPD_ERR_DEVICE: return "device reported an error status";
     case SPD_ERR_ALIGN: return "a field pointer is not 16-byte aligned";
     case SPD_ERR_NOALLOC_LIMIT:
       return "instance has more latitudes than spd_fwd_noalloc's fixed scratch holds "

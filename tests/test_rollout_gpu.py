@@ -64,14 +64,28 @@ def one_column(inst, i, j):
     return sub
 
 
-@pytest.mark.parametrize("kx", [8, 16])
-def test_single_column_rollout_matches_float64_host(host, kx):
-    inst = pkg.synthetic.land_instance(700 + kx, 16, 8, kx)
-    tend, data, S = run_oracle(inst)
-    vg, pr = structs(pkg, inst)
-    rng = np.random.default_rng(kx)
+def rollout_columns_against_host(host, inst, columns, seed, params=None):
+    """48-step rollout VJPs of single-column instances cut from ``inst`` on the GPU (float32)
+    and on the host (float64), with the parameter overrides ``params`` ({"group.name": value});
+    returns the normwise errors of the state gradients by field and of the 12 parameter
+    gradients."""
+    kx = inst.kx
+    if params:
+        P = pkg.Parameters.default().with_values(
+            **{k.replace(".", "__"): v for k, v in params.items()})
+        from oracle import speedy_oracle as O
+        tend, data = O.compute_tendencies(*inst.oracle_args(O.default_parameters(**params)))
+        S = int(sum(1 << int(l) for l in np.nonzero(O.cloud_top_level_set(
+            data.shortwave_rad.icltop, kx))[0]))
+    else:
+        P = pkg.Parameters.default()
+        tend, data, S = run_oracle(inst)
+    phys = pkg.SpeedyPhysics(P)
+    vg, _ = structs(pkg, inst)
+    pr = P.to_struct()
+    rng = np.random.default_rng(seed)
     G, H, PG, PH = [], [], [], []
-    for (i, j) in [(1, 2), (5, 3), (9, 6), (13, 1), (3, 7), (11, 4)]:
+    for (i, j) in columns:
         sub = one_column(inst, i, j)
         st, fo, ge, da = pkg.instance_to_device(sub, "cuda")
         ctv = np.zeros((4, kx))
@@ -79,7 +93,7 @@ def test_single_column_rollout_matches_float64_host(host, kx):
         ctv[2], ctv[3] = rng.normal(size=kx), rng.normal(size=kx)
         ct = pkg.PhysicsTendency(*(torch.tensor(ctv[n], dtype=torch.float32, device="cuda")
                                    .view(kx, 1, 1) for n in range(4)))
-        _, g, gp = R.rollout_vjp(None, st, fo, ge, da, ct, nsteps=48)
+        _, g, gp = R.rollout_vjp(phys, st, fo, ge, da, ct, nsteps=48)
         h = column_of(inst, data, S, i, j, 1 | 2 | 4)
         x0 = np.zeros(51)
         x0[:kx], x0[16:16 + kx], x0[32:32 + kx] = inst.t[:, i, j], inst.q[:, i, j], inst.phi[:, i, j]
@@ -104,6 +118,29 @@ def test_single_column_rollout_matches_float64_host(host, kx):
     errs = {k: float(np.max(np.abs(G[:, s] - H[:, s])) / max(np.max(np.abs(H[:, s])), 1e-30))
             for k, s in segs.items()}
     perr = float(np.max(np.abs(PG - PH)) / np.max(np.abs(PH)))
+    return errs, perr
+
+
+@pytest.mark.parametrize("kx", [8, 16])
+def test_single_column_rollout_matches_float64_host(host, kx):
+    inst = pkg.synthetic.land_instance(700 + kx, 16, 8, kx)
+    errs, perr = rollout_columns_against_host(
+        host, inst, [(1, 2), (5, 3), (9, 6), (13, 1), (3, 7), (11, 4)], seed=kx)
     print("normwise errors", errs, "params", perr)
+    assert all(e <= 1e-4 for e in errs.values()), errs
+    assert perr <= 1e-4, perr
+
+
+def test_t42_rollout_with_perturbed_parameters_matches_float64_host(host):
+    """The adjoint workload's rollout: columns of the T42 instance (128 x 64, 8 levels, land and
+    sea ice) with the 12 differentiated parameters scaled by seeded U(0.8, 1.2) factors, a
+    48-step rollout VJP with checkpoints every 8 steps on the GPU against the float64 host
+    rollout, column by column."""
+    from tests.test_adjoint_config2_gpu import perturbed_parameters
+    inst = pkg.synthetic.land_instance(42, 128, 64, 8, sst_noise=1.5)
+    params = perturbed_parameters(pkg, seed=6)
+    cols = [(3, 5), (17, 60), (40, 31), (77, 12), (101, 47), (126, 20), (64, 2), (90, 58)]
+    errs, perr = rollout_columns_against_host(host, inst, cols, seed=42, params=params)
+    print("T42 perturbed rollout normwise errors", errs, "params", perr)
     assert all(e <= 1e-4 for e in errs.values()), errs
     assert perr <= 1e-4, perr
