@@ -29,10 +29,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per column of the dominant kernel (ensemble_fused) and its warp
-# instructions per launch, from one ncu capture each (the commands and figures are in the
-# profiles/ summaries named for the kernel and workload); None until captured.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": None, "t425": None}
-NCU_WARP_INSTRUCTIONS = {"ensemble": None, "t425": None, "adjoint_t170": 117031373.0}
+# instructions per launch, from one ncu capture each (the summaries under profiles/ give the
+# commands): T425 from a --set full capture of one plain call (196.7 MB read + 170.4 MB
+# written, 237.4 M warp instructions); the ensemble from the dram__bytes / inst_executed
+# metrics of one fused launch of the benchmark's step; the adjoint (ensemble_adjoint, T170
+# with 16 levels) from a --set full capture of one VJP.  Part of each launch's writes is still
+# in L2 when the kernel ends, so the write share reads low.
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": None,
+                          "t425": (196.710912e6 + 170.406912e6) / 819200}
+NCU_WARP_INSTRUCTIONS = {"ensemble": None, "t425": 237409209.0,
+                         "adjoint_t170": 117031373.0}
 
 
 def parse_args():
