@@ -165,10 +165,11 @@ int spd_fwd(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 
 /* Timing hook (no reference counterpart): spd_fwd, recording `event` (a cudaEvent_t, or NULL)
  * on `stream` between its two launches, so that a caller can time them separately with
- * events.  With an event the launches run in plain stream order; without one (and in spd_fwd)
- * the second launch is a programmatic dependent launch: its blocks start as the first one's
- * retire and run the first half of their columns, then wait on the device for the first
- * launch's completion before reading the level set and the solar table. */
+ * events: after the fused launch (before the fixup) when the call predicts the level set,
+ * after the level-set launch (before the fused one) under SPD_NO_SPECULATION.  With an event
+ * the launches run in plain stream order; without one (and in spd_fwd) the second launch is a
+ * programmatic dependent launch: its blocks start as the first one's retire and wait on the
+ * device for the first launch's completion before reading what it wrote. */
 int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t* params,
                    const spd_inputs_t* in, const spd_outputs_t* out, void* scratch,
                    size_t scratch_bytes, void* stream, void* event);
@@ -245,8 +246,9 @@ int spd_vjp(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_params_t
 
 /* ----------------------------------------------------------------------------------------- */
 /* Batched ragged ensemble: many instances ("members") of mixed resolution and level count,  */
-/* e.g. a forecast ensemble or a set of independent grids, in one pair of persistent launches  */
-/* (first half of every member's columns, then the second half of every member's columns).   */
+/* e.g. a forecast ensemble or a set of independent grids, in one fused launch over every      */
+/* member's columns (and a fixup launch that redoes the members whose predicted level set       */
+/* missed, or a level-set launch first under SPD_NO_SPECULATION).  Each                        */
 /* member gives the same results as spd_fwd on it alone.  There is no reference counterpart   */
 /* for the batching itself; per member it replaces SpeedyPhysics.compute_tendencies           */
 /* (speedy_physics.py:88-127).                                                               */
@@ -296,8 +298,8 @@ int spd_ensemble_fwd(const spd_class_t* classes, int nclasses, void* plan_device
                      const spd_plan_info_t* info, int grid_blocks, void* stream);
 
 /* Timing hook (no reference counterpart): spd_ensemble_fwd, recording `event` (a cudaEvent_t,
- * or NULL) on `stream` between its two launches (the level sets and the columns), which then
- * run in plain stream order (see spd_fwd_marked). */
+ * or NULL) on `stream` between its two launches (see spd_fwd_marked), which then run in plain
+ * stream order. */
 int spd_ensemble_fwd_marked(const spd_class_t* classes, int nclasses, void* plan_device,
                             const spd_plan_info_t* info, int grid_blocks, void* stream,
                             void* event);

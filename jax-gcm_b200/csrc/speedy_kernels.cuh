@@ -44,8 +44,8 @@ __device__ __forceinline__ void or_level_set_warp(uint32_t bit, uint32_t* S) {
   }
 }
 
-// Cloud-top level bit of column c from registers (the adjoint's pre-pass; the forward takes it
-// from its first half).
+// Cloud-top level bit of column c from registers (the adjoint's pre-pass; the forward forms it
+// from its own first half, column_first).
 template <int KX>
 __device__ __forceinline__ uint32_t prepass_column(const Consts& K, const spd_inputs_t& in,
                                                    int c, int C) {

@@ -17,7 +17,7 @@ layer a forecast service would put in front of the physics:
   one packed buffer from pinned host memory on a copy stream, and stay on the device while any
   request uses them (and afterwards, until evicted).
 * Continuous batching.  Requests admitted while earlier batches run are merged into the next
-  batch of their kind: one ragged-ensemble launch pair over all their members
+  batch of their kind: one ragged-ensemble launch over all their members
   (``spd_ensemble_fwd`` for tendencies, ``spd_ensemble_vjp`` for VJPs), enqueued while up to
   ``max_inflight`` earlier batches of that kind are still on the device.  VJP batches run on
   their own stream, so their work overlaps the tendency batches on the device, and uploads
