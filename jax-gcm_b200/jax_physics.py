@@ -139,7 +139,10 @@ class SpeedyPhysicsB200:
 
     def _statics(self, geometry, lfluxland):
         kx, ix, il = geometry.nodal_shape
-        d = _lib.Desc(kx, ix, il, flags_of(self.parameters, lfluxland), 0.0, 0, 0,
+        # XLA allocates each call's scratch afresh, so no call can predict the cloud-top level
+        # set from the previous one: form it first (SPD_NO_SPECULATION), one light launch
+        flags = flags_of(self.parameters, lfluxland) | _lib.SPD_NO_SPECULATION
+        d = _lib.Desc(kx, ix, il, flags, 0.0, 0, 0,
                       int(self.parameters.forcing.co2_year_ref), 1800.0, 1.0)
         lib = _lib.load()
         return (d, vgrid_struct(geometry), int(lib.spd_fwd_scratch_bytes(C.byref(d))),
