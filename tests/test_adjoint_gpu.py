@@ -7,7 +7,10 @@ max(1e-4, 3x the host float32 VJP's own largest distance from float64) of the fi
 column outside that bar is a branch flip (a convection, condensation or cloud threshold
 decided differently in float32) and is explained when the GPU agrees with the host float32
 VJP there, or when the host float32 VJP is itself outside the bar; at most 1 % of the columns
-may flip and none may be unexplained.
+may flip and none may be unexplained.  Parameter gradients: each of the 12 within 1e-4
+relative of the float64 host sum over the columns (the flipped columns' contributions taken
+from the float32 host), above a floor of 1e-2 of the sum of the contributions' magnitudes for
+sums that cancel.
 """
 import importlib
 
@@ -74,7 +77,7 @@ def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify, oro):
     flags = _flags(inst) | (16 if verify else 0) | (32 if oro else 0)
     h64 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
     h32 = {k: np.zeros_like(v) for k, v in g_gpu.items()}
-    p64 = np.zeros(12)
+    pc = {False: np.zeros((inst.ix, inst.il, 12)), True: np.zeros((inst.ix, inst.il, 12))}
     for i in range(inst.ix):
         for j in range(inst.il):
             h = column_of(inst, data, S, i, j, flags)
@@ -91,9 +94,9 @@ def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify, oro):
                 dst["t"][:, i, j], dst["q"][:, i, j], dst["phi"][:, i, j] = g["t"], g["q"], g["phi"]
                 dst["psa"][i, j] = g["psa"]
                 dst["u"][-1, i, j], dst["v"][-1, i, j] = g["u"], g["v"]
-                if not f32:
-                    p64 += g["params"]
+                pc[f32][i, j] = g["params"]
     report = {}
+    flipped = np.zeros((inst.ix, inst.il), bool)
     for k in ("t", "q", "phi", "psa", "u", "v"):
         scale = max(np.max(np.abs(h64[k])), 1e-30)
         e_gpu = np.abs(g_gpu[k] - h64[k]) / scale
@@ -108,9 +111,18 @@ def test_gpu_vjp_matches_host(pkg, host, kx, seed, lfluxland, verify, oro):
         unexplained = bad & ~agrees32 & ~flips32
         assert unexplained.sum() == 0, (k, report[k], np.argwhere(unexplained))
         assert bad.sum() <= max(2, 0.01 * inst.ix * inst.il), (k, report[k], bad.sum())
+        flipped |= bad
     print(inst.name, report)
-    rel = np.abs(p_gpu - p64) / np.maximum(np.abs(p64), 1e-30)
-    assert np.sum(rel > 1e-3) <= 1, (p_gpu, p64)
+    # the float64 sum, with the flipped columns' contributions from the float32 host (the GPU
+    # takes their float32 branch)
+    p64 = np.where(flipped[..., None], pc[True], pc[False]).sum(axis=(0, 1))
+    p64_abs = np.abs(pc[False]).sum(axis=(0, 1))  # the magnitude of the summed contributions
+    # every parameter gradient within 1e-4 relative; where the column contributions cancel to
+    # below 1e-2 of their magnitudes (a sum's condition number above 100), the floor is 1e-2 of
+    # that magnitude
+    rel = np.abs(p_gpu - p64) / np.maximum(np.maximum(np.abs(p64), 1e-2 * p64_abs), 1e-30)
+    print("parameter gradients, relative error", np.array2string(rel, precision=1))
+    assert np.all(rel <= 1e-4), (p_gpu, p64, rel)
 
 
 def test_autograd_through_torch_op(pkg):
