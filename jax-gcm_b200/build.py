@@ -16,7 +16,7 @@ SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu", "csrc/speedy_ensemble
            "csrc/speedy_adjoint.cu", "csrc/held_suarez.cu"]
 HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
            "csrc/speedy_kernels.cuh", "csrc/speedy_ensemble.cuh", "csrc/speedy_ad.h",
-           "csrc/speedy_generic.h", "csrc/speedy_vjp.h",
+           "csrc/speedy_generic.h", "csrc/speedy_vjp.h", "csrc/speedy_pk.cuh",
            "../include/speedy_b200.h"]
 OUT = os.path.join(HERE, "libspeedy_b200.so")
 OBJ_DIR = os.path.join(HERE, "_build")

@@ -36,6 +36,7 @@
 
 #include "speedy_column.cuh"
 #include "speedy_derived.h"
+#include "speedy_pk.cuh"
 
 namespace spd {
 
@@ -105,18 +106,29 @@ __device__ __forceinline__ void st4a_at(const Consts& K, const Lv& T, int k, flo
   }
 }
 
-// Longwave band energy fractions (radset, longwave_radiation.py:204-226) times (1 - epslw).
-__device__ __forceinline__ void radset_w(float temp, float w, float fb[4]) {
+// Longwave band energy fractions (radset, longwave_radiation.py:204-226) times (1 - epslw), as
+// the band pairs (0, 1) and (2, 3); bands 1 and 2 share their packed quadratic.
+__device__ __forceinline__ void radset_w(float temp, float w, float2& fb01, float2& fb23) {
   const float j = fminf(fmaxf(temp, 200.0f), 320.0f);
-  const float f1 = 0.148f - 3.0e-6f * sq(j - 247.0f);
-  const float f2 = 0.356f - 5.2e-6f * sq(j - 282.0f);
+  const float2 d = pk_sub(bc(j), pk(247.0f, 282.0f));
+  const float2 f12 = pk_sub_sep(pk(0.148f, 0.356f), pk_mul(pk(3.0e-6f, 5.2e-6f), pk_mul(d, d)));
   const float f3 = 0.314f + 1.0e-5f * sq(j - 315.0f);
-  const float f0 = 1.0f - (((0.0f + f1) + f2) + f3);
-  fb[0] = w * f0;
-  fb[1] = w * f1;
-  fb[2] = w * f2;
-  fb[3] = w * f3;
+  const float f0 = 1.0f - (((0.0f + f12.x) + f12.y) + f3);
+  fb01 = pk_mul(bc(w), pk(f0, f12.x));
+  fb23 = pk_mul(bc(w), pk(f12.y, f3));
 }
+
+// One band pair's flux recurrence (longwave_radiation.py:99-104 downward, 160-166 upward, the
+// sign sg of the gradient term): tau * fl + emis * (fb * (s0 +/- emis * s1)), emis = 1 - tau.
+template <bool kDown>
+__device__ __forceinline__ float2 lw_step(float2 tau, float2 fl, float2 fb, float s0, float s1) {
+  const float2 emis = pk_sub(bc(1.0f), tau);
+  const float2 es1 = pk_mul(emis, bc(s1));
+  const float2 src = kDown ? pk_add_sep(bc(s0), es1) : pk_sub_sep(bc(s0), es1);
+  return pk_add_sep(pk_mul(tau, fl), pk_mul(emis, pk_mul(fb, src)));
+}
+
+__device__ __forceinline__ float sum4(float2 a, float2 b) { return ((a.x + a.y) + b.x) + b.y; }
 
 // First half of the column: humidity, convection, large-scale condensation and clouds, with
 // every level loop fully unrolled so that the level arrays live in registers.  In: the state T,
@@ -397,17 +409,25 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       add_sw(1, d1_band1);
       add_sw(1, prev * (1.0f - tau1));
     }
+    // Levels 2..kx-1, two bands and two absorbed pieces in packed pairs: the exponents
+    // (m x_k, m abswv2) with m = -psaz dhs_k, then (prev t0, prev (1 - r)) x ((1 - r), (1 - t0))
+    // = (f1, d), (prev2 tau1, prev2 (1 - tau1)), and both pieces' scalings.
 #pragma unroll 4
     for (int k = 2; k < KX; ++k) {
-      const float prev = f1, r = W[k], t0 = tau0_at(k);
-      f1 = prev * t0 * (1.0f - r);
-      const float d = prev * (1.0f - r) * (1.0f - t0);
+      const float prev = f1, r = W[k];
+      const float cl = (k < KX - 1 && k >= icltop) ? acloud : 0.0f;
+      const float m = -psaz * vg.dhs[k];
+      const float2 ex = pk_mul(bc(m), pk(D.abs1[k] + p.abswv1 * Q[k] + cl, p.abswv2));
+      const float t0 = texp(ex.x), tau1 = texp(ex.y * Q[k]);
+      const float2 om = pk_sub(bc(1.0f), pk(r, t0));
+      const float2 fd = pk_mul(pk_mul(bc(prev), pk(t0, om.x)), om);
+      f1 = fd.x;
       W[k] = r * prev;
-      const float tau1 = texp(-psaz * vg.dhs[k] * p.abswv2 * Q[k]);
       const float prev2 = f2;
-      f2 = prev2 * tau1;
-      add_sw(k, d);
-      add_sw(k, prev2 * (1.0f - tau1));
+      const float2 f2e = pk_mul(bc(prev2), pk(tau1, 1.0f - tau1));
+      f2 = f2e.x;
+      const float2 g = pk_mul(pk_mul(pk(fd.y, f2e.y), bc(vg.grdscp[k])), bc(rps));
+      DT[k] = (DT[k] + (gate ? g.x : 0.0f)) + (gate ? g.y : 0.0f);
     }
     rsds = f1 + f2;
     float up = f1 * albsfc;
@@ -429,59 +449,53 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
 
   // ---- longwave transmissivities of level k (shortwave_radiation.py:174-206) ---------------
   const float acl1 = cloudc * p.ablcl1, acl2 = cloudc * p.ablcl2;
-  auto lw_tau = [&](int k, float tau[4]) {
-    const float qk = Q[k];
-    float a0 = p.ablwin, a2 = p.ablwv1 * qk, a3 = p.ablwv2 * qk;
-    if (k == 0) {
-      a2 = 0.0f;
-      a3 = 0.0f;
-    }
+  // (-a * psa) * dhs, formed as -((a * psa) * dhs): the same bits (round-to-nearest is
+  // symmetric in sign)
+  auto lw_tau = [&](int k, float2& t01, float2& t23) {
+    float2 a23 = pk_mul(pk(p.ablwv1, p.ablwv2), bc(Q[k]));
+    float a0 = p.ablwin;
+    if (k == 0) a23 = bc(0.0f);
     if (k >= 2 && k <= KX - 2) {
       a0 = a0 + ((k > icltop) ? acl1 : acl2);
-      a2 = fmaxf(a2, acl2);
-      a3 = fmaxf(a3, acl2);
+      a23 = pk(fmaxf(a23.x, acl2), fmaxf(a23.y, acl2));
     }
-    tau[0] = texp(-a0 * psa * vg.dhs[k]);
-    tau[1] = texp(-D.ablco2 * psa * vg.dhs[k]);
-    tau[2] = texp(-a2 * psa * vg.dhs[k]);
-    tau[3] = texp(-a3 * psa * vg.dhs[k]);
+    const float2 pd = bc(vg.dhs[k]);
+    const float2 x01 = pk_mul(pk_mul(pk(a0, D.ablco2), bc(psa)), pd);
+    const float2 x23 = pk_mul(pk_mul(a23, bc(psa)), pd);
+    t01 = pk(texp(-x01.x), texp(-x01.y));
+    t23 = pk(texp(-x23.x), texp(-x23.y));
   };
   auto add_lw = [&](int k, float d) { DT[k] = DT[k] + d * vg.grdscp[k] * rps; };
 
   // ---- get_downward_longwave_rad_fluxes (longwave_radiation.py:13-117) ---------------------
   float rlds;
   {
-    float fl[4], fb[4], tau[4], s0, s1;
+    float2 fl01, fl23, fb01, fb23, t01, t23;
+    float s0, s1;
     st4a_at<KX>(K, T, 0, s0, s1);
-    radset_w(T[0], D.w_lw, fb);
-    lw_tau(0, tau);
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const float emis = 1.0f - tau[b];
-      fl[b] = emis * (fb[b] * (s0 + emis * s1));
+    radset_w(T[0], D.w_lw, fb01, fb23);
+    lw_tau(0, t01, t23);
+    {  // the top level: no flux from above; bands 2 and 3 start at zero
+      const float2 emis = pk_sub(bc(1.0f), t01);
+      fl01 = pk_mul(emis, pk_mul(fb01, pk_add_sep(bc(s0), pk_mul(emis, bc(s1)))));
+      fl23 = bc(0.0f);
     }
-    fl[2] = 0.0f;
-    fl[3] = 0.0f;
-    float sprev = sum4(fl);
+    float sprev = sum4(fl01, fl23);
     add_lw(0, 0.0f + (-sprev));
 #pragma unroll 4
     for (int k = 1; k < KX; ++k) {
       st4a_at<KX>(K, T, k, s0, s1);
-      radset_w(T[k], D.w_lw, fb);
-      lw_tau(k, tau);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const float emis = 1.0f - tau[b];
-        fl[b] = tau[b] * fl[b] + emis * (fb[b] * (s0 + emis * s1));
-      }
-      const float sk = sum4(fl);
+      radset_w(T[k], D.w_lw, fb01, fb23);
+      lw_tau(k, t01, t23);
+      fl01 = lw_step<true>(t01, fl01, fb01, s0, s1);
+      fl23 = lw_step<true>(t23, fl23, fb23, s0, s1);
+      const float sk = sum4(fl01, fl23);
       float d = 0.0f + (-(sk - sprev));
       if (k == KX - 1) d = d + (-(D.corlw_f * s0));
       add_lw(k, d);
       sprev = sk;
     }
-    const float ef[4] = {p.emisfc * fl[0], p.emisfc * fl[1], p.emisfc * fl[2], p.emisfc * fl[3]};
-    rlds = sum4(ef);
+    rlds = sum4(pk_mul(bc(p.emisfc), fl01), pk_mul(bc(p.emisfc), fl23));
     rlds = rlds + D.corlw_f * s0;
   }
   o.rlds = rlds;
@@ -582,24 +596,21 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
   // ---- get_upward_longwave_rad_fluxes (longwave_radiation.py:119-202) ---------------------
   {
     o.rlns = rlus2 - rlds;
-    float fb[4], fl[4], tau[4], s0, s1;
-    radset_w(tsfc, D.w_lw, fb);
-    const float fsw[4] = {flux_sw0, flux_sw1, 0.0f, 0.0f};
-#pragma unroll
-    for (int b = 0; b < 4; ++b) fl[b] = fb[b] * rlus2 + D.refsfc * fsw[b];
-    float sk = sum4(fl);
+    float2 fb01, fb23, fl01, fl23, t01, t23;
+    float s0, s1;
+    radset_w(tsfc, D.w_lw, fb01, fb23);
+    fl01 = pk_add_sep(pk_mul(fb01, bc(rlus2)), pk_mul(bc(D.refsfc), pk(flux_sw0, flux_sw1)));
+    fl23 = pk_add_sep(pk_mul(fb23, bc(rlus2)), pk_mul(bc(D.refsfc), bc(0.0f)));
+    float sk = sum4(fl01, fl23);
     float d_last = p.epslw * rlus2;  // dfabs[kx-1] += epslw*rlus before the scan
 #pragma unroll 4
     for (int k = KX - 1; k >= 1; --k) {
       st4a_at<KX>(K, T, k, s0, s1);
-      radset_w(T[k], D.w_lw, fb);
-      lw_tau(k, tau);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const float emis = 1.0f - tau[b];
-        fl[b] = tau[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1));
-      }
-      const float skm1 = sum4(fl);
+      radset_w(T[k], D.w_lw, fb01, fb23);
+      lw_tau(k, t01, t23);
+      fl01 = lw_step<false>(t01, fl01, fb01, s0, s1);
+      fl23 = lw_step<false>(t23, fl23, fb23, s0, s1);
+      const float skm1 = sum4(fl01, fl23);
       float d = (sk - skm1);
       if (k == KX - 1) d = d_last + d;
       if (k >= 2) add_lw(k, d);
@@ -609,20 +620,16 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
     st4a_at<KX>(K, T, 0, s0, s1);
     float s0b, s1b;
     st4a_at<KX>(K, T, 1, s0b, s1b);
-    radset_w(T[0], D.w_lw, fb);
-    lw_tau(0, tau);
-    float top[4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const float emis = 1.0f - tau[b];
-      top[b] = (b < 2) ? tau[b] * fl[b] + emis * (fb[b] * (s0 - emis * s1)) : fl[b];
-    }
+    radset_w(T[0], D.w_lw, fb01, fb23);
+    lw_tau(0, t01, t23);
+    const float2 top01 = lw_step<false>(t01, fl01, fb01, s0, s1);  // bands 2, 3 pass level 0
     const float stratc0 = z.stratz * psa, stratc1 = D.eps1 * psa;
     const float corlw1 = vg.dhs[0] * stratc1 * s0 + stratc0;
     const float corlw2 = vg.dhs[1] * stratc1 * s0b;
-    add_lw(0, ((fl[0] - top[0]) + (fl[1] - top[1])) + (-corlw1));
+    const float2 dtop = pk_sub(fl01, top01);
+    add_lw(0, (dtop.x + dtop.y) + (-corlw1));
     add_lw(1, d_last + (-corlw2));
-    o.ftop_lw = (corlw1 + corlw2) + sum4(top);
+    o.ftop_lw = (corlw1 + corlw2) + sum4(top01, fl23);
   }
 
   // ---- get_vertical_diffusion_tend (vertical_diffusion.py:10-136) -------------------------
