@@ -30,15 +30,15 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per column of the dominant kernel (ensemble_fused) and its warp
 # instructions per launch, from one ncu capture each (the summaries under profiles/ give the
-# commands): T425 from a --set full capture of one plain call (196.7 MB read + 170.4 MB
-# written, 237.4 M warp instructions); the ensemble from the dram__bytes / inst_executed
-# metrics of one fused launch of the benchmark's step (96.2 MB read + 58.5 MB written, 113.2 M
+# commands): T425 from a --set full capture of one plain call (196.8 MB read + 171.6 MB
+# written, 221.8 M warp instructions); the ensemble from the dram__bytes / inst_executed
+# metrics of one fused launch of the benchmark's step (96.2 MB read + 58.9 MB written, 105.9 M
 # warp instructions; one block per tile, the autotuner's pick); the adjoint (ensemble_adjoint, T170
 # with 16 levels) from a --set full capture of one VJP.  Part of each launch's writes is still
 # in L2 when the kernel ends, so the write share reads low.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.213760e6 + 58.501120e6) / 466944,
-                          "t425": (196.710912e6 + 170.406912e6) / 819200}
-NCU_WARP_INSTRUCTIONS = {"ensemble": 113159373.0, "t425": 237409209.0,
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.207104e6 + 58.852864e6) / 466944,
+                          "t425": (196.762624e6 + 171.640064e6) / 819200}
+NCU_WARP_INSTRUCTIONS = {"ensemble": 105899680.0, "t425": 221814507.0,
                          "adjoint_t170": 117031373.0}
 
 
