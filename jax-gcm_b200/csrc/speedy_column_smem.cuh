@@ -98,12 +98,34 @@ __device__ __forceinline__ void st4a_at(const Consts& K, const Lv& T, int k, flo
     s1 = 0.0f;
   } else {
     const float t = T[k];
-    const float grad = (k < KX - 1) ? 0.5f * fmaxf(th(k) - th(k - 1), 0.0f)
-                                    : fmaxf(t - th(KX - 2), 0.0f);
+    float grad;
+    if (k < KX - 1) {  // th(k) and th(k - 1) as one pair
+      const float2 tl = pk(T[k], T[k - 1]);
+      const float2 th2 = pk_add_sep(
+          tl, pk_mul(pk(vg.wvi[k][1], vg.wvi[k - 1][1]), pk_sub(pk(T[k + 1], T[k]), tl)));
+      grad = 0.5f * fmaxf(th2.x - th2.y, 0.0f);
+    } else {
+      grad = fmaxf(t - th(KX - 2), 0.0f);
+    }
     const float st3 = kSbc * (t * t * t);
-    s0 = st3 * t;
-    s1 = 4.0f * st3 * grad;
+    const float2 s04 = pk_mul(bc(st3), pk(t, 4.0f));  // (st3 t, 4 st3)
+    s0 = s04.x;
+    s1 = s04.y * grad;
   }
+}
+
+// s0 of st4a_at alone (the same expressions), for the upward pass, which takes s1 from the
+// downward pass.
+template <int KX>
+__device__ __forceinline__ float st4a_s0(const Consts& K, const Lv& T, int k) {
+  if (k <= 1) {
+    float s0, s1;
+    st4a_at<KX>(K, T, k, s0, s1);
+    return s0;
+  }
+  const float t = T[k];
+  const float st3 = kSbc * (t * t * t);
+  return st3 * t;
 }
 
 // Longwave band energy fractions (radset, longwave_radiation.py:204-226) times (1 - epslw), as
@@ -470,6 +492,8 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
   // ---- get_downward_longwave_rad_fluxes (longwave_radiation.py:13-117) ---------------------
   float rlds;
   {
+    // W keeps each level's blackbody gradient term s1 for the upward pass (W is free once the
+    // shortwave is done)
     float2 fl01, fl23, fb01, fb23, t01, t23;
     float s0, s1;
     st4a_at<KX>(K, T, 0, s0, s1);
@@ -485,6 +509,7 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
 #pragma unroll 4
     for (int k = 1; k < KX; ++k) {
       st4a_at<KX>(K, T, k, s0, s1);
+      W[k] = s1;
       radset_w(T[k], D.w_lw, fb01, fb23);
       lw_tau(k, t01, t23);
       fl01 = lw_step<true>(t01, fl01, fb01, s0, s1);
@@ -605,7 +630,8 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
     float d_last = p.epslw * rlus2;  // dfabs[kx-1] += epslw*rlus before the scan
 #pragma unroll 4
     for (int k = KX - 1; k >= 1; --k) {
-      st4a_at<KX>(K, T, k, s0, s1);
+      s0 = st4a_s0<KX>(K, T, k);
+      s1 = W[k];
       radset_w(T[k], D.w_lw, fb01, fb23);
       lw_tau(k, t01, t23);
       fl01 = lw_step<false>(t01, fl01, fb01, s0, s1);
@@ -668,9 +694,10 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       const float dr = rh_n - rh_k;
       const bool cond = (D.vdcond >> k) & 1u;
       const float fq = (dr >= D.drh0v[k] && cond) ? D.fvdiq2v[k] * QS[k] * dr : 0.0f;
-      const float qk = (k == 2) ? (0.0f + fq * D.rsig[k]) : (0.0f + fq * D.rsig[k]) + pend;
+      const float2 fr = pk_mul(bc(fq), pk(D.rsig[k], D.rsig[k + 1]));
+      const float qk = (k == 2) ? (0.0f + fr.x) : (0.0f + fr.x) + pend;
       DQ[k] = DQ[k] + qk;
-      pend = -fq * D.rsig[k + 1];
+      pend = -fr.y;
       rh_k = rh_n;
     }
     DQ[KX - 2] = DQ[KX - 2] + (qt_sh1 + pend);
@@ -685,9 +712,10 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       const float se0 = se_n - p.segrad * (phi_n - phi_k);
       const float fse = (se_k < se0) ? D.fvdise * (se0 - se_k) : 0.0f;
       const float base = (k == KX - 2) ? tt_sh1 : 0.0f;
-      const float tk = (k == 0) ? (base + fse * D.rsig[k]) : (base + fse * D.rsig[k]) + pend_t;
+      const float2 fr = pk_mul(bc(fse), pk(D.rsig[k], D.rsig1[k]));
+      const float tk = (k == 0) ? (base + fr.x) : (base + fr.x) + pend_t;
       DT[k] = DT[k] + tk;
-      cum = cum + fse * D.rsig1[k];
+      cum = cum + fr.y;
       pend_t = -cum;
       se_k = se_n;
       phi_k = phi_n;
