@@ -180,6 +180,16 @@ int spd_fwd_marked(const spd_desc_t* desc, const spd_vgrid_t* vgrid, const spd_p
  * launches. */
 int spd_preload(void);
 
+/* Self-test of the forward's packed float32 arithmetic (no reference counterpart).  The
+ * forward pairs independent float32 operations into sm_100's packed .f32x2 instructions; this
+ * evaluates every packed piece on n seeded inputs per piece and compares it bit for bit with
+ * the scalar expressions it pairs, compiled with the forward's flags.  mismatches (host, 8
+ * entries) receives the count of differing values per piece: longwave recurrence downward and
+ * upward, band fractions, half-level temperatures, blackbody terms, shortwave band 1, band 2,
+ * heating-rate scaling.  All zero is the contract the forward's results rest on.  Synchronous
+ * on the current device's default stream. */
+int spd_selftest_packed(int n, uint32_t seed, unsigned int* mismatches);
+
 /* ----------------------------------------------------------------------------------------- */
 /* Held-Suarez forcing: HeldSuarezPhysics.compute_tendencies                                 */
 /*   (jcm/physics/held_suarez/held_suarez_physics.py:76-101), the reference's second physics */

@@ -166,6 +166,8 @@ def _declare(lib):
     lib.spd_vjp.restype = C.c_int
     lib.spd_preload.argtypes = []
     lib.spd_preload.restype = C.c_int
+    lib.spd_selftest_packed.argtypes = [C.c_int, C.c_uint32, P(C.c_uint)]
+    lib.spd_selftest_packed.restype = C.c_int
     lib.spd_ensemble_vjp_plan_bytes.argtypes = [P(VjpMember), C.c_int]
     lib.spd_ensemble_vjp_plan_bytes.restype = C.c_size_t
     lib.spd_ensemble_vjp_plan.argtypes = [P(Class), C.c_int, P(VjpMember), C.c_int, C.c_void_p,

@@ -13,7 +13,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = ["csrc/speedy_api.cu", "csrc/speedy_noalloc.cu", "csrc/speedy_ensemble.cu",
-           "csrc/speedy_adjoint.cu", "csrc/held_suarez.cu"]
+           "csrc/speedy_adjoint.cu", "csrc/held_suarez.cu", "csrc/speedy_selftest.cu"]
 HEADERS = ["csrc/speedy_column.cuh", "csrc/speedy_column_smem.cuh", "csrc/speedy_derived.h",
            "csrc/speedy_kernels.cuh", "csrc/speedy_ensemble.cuh", "csrc/speedy_ad.h",
            "csrc/speedy_generic.h", "csrc/speedy_vjp.h", "csrc/speedy_pk.cuh",
@@ -33,7 +33,9 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 # measured against the oracles they change nothing (tendencies, precipitation and diagnostics
 # keep their distances at the printed digits; the only values flushed are transmissivities below
 # 1e-38).  The adjoint keeps IEEE arithmetic.
-SOURCE_FLAGS = {"csrc/speedy_ensemble.cu": ["-fmad=false", "-prec-div=false", "-ftz=true"]}
+FORWARD_FLAGS = ["-fmad=false", "-prec-div=false", "-ftz=true"]
+SOURCE_FLAGS = {"csrc/speedy_ensemble.cu": FORWARD_FLAGS,
+                "csrc/speedy_selftest.cu": FORWARD_FLAGS}  # checks the forward's arithmetic
 
 
 def _nvcc():

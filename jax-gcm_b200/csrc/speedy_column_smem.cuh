@@ -82,6 +82,40 @@ __device__ __forceinline__ float se_at(const Lv& T, const Lv& PHI, int k) {
   return kCp * T[k] + PHI[k];
 }
 
+// Packed pieces of the second half, each a pair of the scalar expressions named beside it (the
+// same operations in the same order, so the same bits; checked against those expressions by
+// spd_selftest_packed).
+
+// (th(k), th(k - 1)), th(j) = T[j] + wvi[j][1] (T[j + 1] - T[j]) (longwave_radiation.py:49).
+__device__ __forceinline__ float2 th_pair(float tkm1, float tk, float tkp1, float wk, float wkm1) {
+  const float2 tl = pk(tk, tkm1);
+  return pk_add_sep(tl, pk_mul(pk(wk, wkm1), pk_sub(pk(tkp1, tk), tl)));
+}
+
+// (st3 t, 4 st3) with st3 = sbc t^3: the blackbody term s0 and the factor of s1
+// (longwave_radiation.py:66-68).
+__device__ __forceinline__ float2 bb_pair(float t) {
+  const float st3 = kSbc * (t * t * t);
+  return pk_mul(bc(st3), pk(t, 4.0f));
+}
+
+// Shortwave band 1 through a level: (f1, d) = (prev t0 (1 - r), prev (1 - r) (1 - t0))
+// (shortwave_radiation.py:124, 137).
+__device__ __forceinline__ float2 sw_band1(float prev, float r, float t0) {
+  const float2 om = pk_sub(bc(1.0f), pk(r, t0));
+  return pk_mul(pk_mul(bc(prev), pk(t0, om.x)), om);
+}
+
+// Shortwave band 2 through a level: (prev2 tau1, prev2 (1 - tau1)) (shortwave_radiation.py:141-147).
+__device__ __forceinline__ float2 sw_band2(float prev2, float tau1) {
+  return pk_mul(bc(prev2), pk(tau1, 1.0f - tau1));
+}
+
+// Two absorbed pieces scaled to heating rates: (a g rps, b g rps).
+__device__ __forceinline__ float2 sw_scale(float a, float b, float g, float rps) {
+  return pk_mul(pk_mul(pk(a, b), bc(g)), bc(rps));
+}
+
 // Blackbody emission st4a[k][0..1] (longwave_radiation.py:42-68), from the level temperatures.
 template <int KX>
 __device__ __forceinline__ void st4a_at(const Consts& K, const Lv& T, int k, float& s0,
@@ -100,15 +134,12 @@ __device__ __forceinline__ void st4a_at(const Consts& K, const Lv& T, int k, flo
     const float t = T[k];
     float grad;
     if (k < KX - 1) {  // th(k) and th(k - 1) as one pair
-      const float2 tl = pk(T[k], T[k - 1]);
-      const float2 th2 = pk_add_sep(
-          tl, pk_mul(pk(vg.wvi[k][1], vg.wvi[k - 1][1]), pk_sub(pk(T[k + 1], T[k]), tl)));
+      const float2 th2 = th_pair(T[k - 1], T[k], T[k + 1], vg.wvi[k][1], vg.wvi[k - 1][1]);
       grad = 0.5f * fmaxf(th2.x - th2.y, 0.0f);
     } else {
       grad = fmaxf(t - th(KX - 2), 0.0f);
     }
-    const float st3 = kSbc * (t * t * t);
-    const float2 s04 = pk_mul(bc(st3), pk(t, 4.0f));  // (st3 t, 4 st3)
+    const float2 s04 = bb_pair(t);  // (st3 t, 4 st3)
     s0 = s04.x;
     s1 = s04.y * grad;
   }
@@ -441,14 +472,13 @@ __device__ void column_second(const ConstsD& C, float* sm, const SurfaceIn& s, c
       const float m = -psaz * vg.dhs[k];
       const float2 ex = pk_mul(bc(m), pk(D.abs1[k] + p.abswv1 * Q[k] + cl, p.abswv2));
       const float t0 = texp(ex.x), tau1 = texp(ex.y * Q[k]);
-      const float2 om = pk_sub(bc(1.0f), pk(r, t0));
-      const float2 fd = pk_mul(pk_mul(bc(prev), pk(t0, om.x)), om);
+      const float2 fd = sw_band1(prev, r, t0);
       f1 = fd.x;
       W[k] = r * prev;
       const float prev2 = f2;
-      const float2 f2e = pk_mul(bc(prev2), pk(tau1, 1.0f - tau1));
+      const float2 f2e = sw_band2(prev2, tau1);
       f2 = f2e.x;
-      const float2 g = pk_mul(pk_mul(pk(fd.y, f2e.y), bc(vg.grdscp[k])), bc(rps));
+      const float2 g = sw_scale(fd.y, f2e.y, vg.grdscp[k], rps);
       DT[k] = (DT[k] + (gate ? g.x : 0.0f)) + (gate ? g.y : 0.0f);
     }
     rsds = f1 + f2;

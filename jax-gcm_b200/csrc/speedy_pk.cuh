@@ -2,8 +2,9 @@
 // operations in one instruction.  Each lane is rounded to nearest on its own, exactly like the
 // scalar instruction it replaces, so a packed expression gives the same bits as the two scalar
 // expressions it pairs.  The lanes flush subnormal results to zero (.ftz), like the scalar
-// arithmetic of the translation unit that instantiates the forward kernels (speedy_ensemble.cu,
-// compiled with -ftz=true); code built without -ftz must not use these.
+// arithmetic of the translation units that use them (speedy_ensemble.cu, the forward kernels,
+// and speedy_selftest.cu, their check; both compiled with -ftz=true); code built without -ftz
+// must not use these.
 //
 // One rule keeps the bits: ptxas contracts a packed add or subtract of a packed product into a
 // fused multiply-add, whatever the rounding modifiers and -fmad say (measured on B200: the
