@@ -128,7 +128,11 @@ class ForcingData:
         return f
 
     def day_slice(self, day):
-        """tree_index_3d(forcing, day) (jcm/utils.py:104-108): 3-D daily fields -> 2-D."""
+        """tree_index_3d(forcing, day) (jcm/utils.py:104-108): 3-D daily fields -> 2-D.  Forcing
+        whose fields are all 2-D already is returned as it is."""
+        names = ("alb0", "sice_am", "snowc_am", "soilw_am", "stl_am", "sea_surface_temperature")
+        if all(getattr(self, n).dim() == 2 for n in names):
+            return self
         out = {}
         for n in ("alb0", "sice_am", "snowc_am", "soilw_am", "stl_am", "sea_surface_temperature"):
             a = getattr(self, n)
@@ -427,6 +431,13 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+def current_raw_stream(device_index):
+    """The current CUDA stream of a device as a raw handle (torch's own fast path where it has
+    one; torch.cuda.current_stream otherwise)."""
+    f = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    return f(device_index) if f is not None else torch.cuda.current_stream(device_index).cuda_stream
+
+
 class SpeedyPhysics(Physics):
     """SPEEDY physics on the B200 (speedy_physics.py:34-132).
 
@@ -459,6 +470,7 @@ class SpeedyPhysics(Physics):
         self.diagnostics = diagnostics
         self._pstruct = self.parameters.to_struct()
         self._scratch = {}
+        self._day = (None, 0)  # (tyear, model day) of the last call
 
     def desc(self, geometry, date, lfluxland):
         kx, ix, il = geometry.nodal_shape
@@ -507,11 +519,14 @@ class SpeedyPhysics(Physics):
         t = state.temperature
         if tuple(t.shape) != (kx, ix, il):
             raise ValueError(f"state shape {tuple(t.shape)} does not match geometry {(kx, ix, il)}")
-        dev = t.device
-        if dev.type != "cuda":
+        if not t.is_cuda:
             raise RuntimeError("SpeedyPhysics runs on CUDA tensors only (no CPU path)")
-        _lib.preload(dev.index if dev.index is not None else torch.cuda.current_device())
-        f2 = forcing.day_slice(date.model_day())
+        dev = t.device
+        didx = t.get_device()
+        _lib.preload(didx)
+        if self._day[0] != date.tyear:
+            self._day = (date.tyear, date.model_day())
+        f2 = forcing.day_slice(self._day[1])
         tensors = dict(u_wind=state.u_wind, v_wind=state.v_wind, temperature=state.temperature,
                        specific_humidity=state.specific_humidity,
                        geopotential=state.geopotential,
@@ -521,9 +536,12 @@ class SpeedyPhysics(Physics):
                        sea_surface_temperature=f2.sea_surface_temperature, fmask=geometry.fmask,
                        orog=geometry.orog, phis0=geometry.phis0, sia=geometry.sia,
                        coa=geometry.coa)
-        for k, v in tensors.items():
-            if v.dtype != torch.float32 or not v.is_contiguous() or v.device != dev:
-                tensors[k] = v.to(device=dev, dtype=torch.float32).contiguous()
+        ptrs = []
+        for k in _lib.INPUT_FIELDS:
+            v = tensors[k]
+            if v.dtype is not torch.float32 or not v.is_contiguous() or v.get_device() != didx:
+                v = tensors[k] = v.to(device=dev, dtype=torch.float32).contiguous()
+            ptrs.append(v.data_ptr())
         if out is None:
             e3 = lambda: torch.empty((kx, ix, il), dtype=torch.float32, device=dev)
             e2 = lambda: torch.empty((ix, il), dtype=torch.float32, device=dev)
@@ -534,14 +552,14 @@ class SpeedyPhysics(Physics):
                     out[n] = e2()
                 out["iptop"] = torch.empty((ix, il), dtype=torch.int32, device=dev)
                 out["icltop"] = torch.empty((ix, il), dtype=torch.int32, device=dev)
-        inp = _lib.Inputs(**{k: tensors[k].data_ptr() for k in _lib.INPUT_FIELDS})
-        outs = _lib.Outputs(**{k: (out[k].data_ptr() if k in out else None)
-                               for k in _lib.OUTPUT_FIELDS})
+        inp = _lib.Inputs(*ptrs)
+        outs = _lib.Outputs(*[out[k].data_ptr() if k in out else None
+                              for k in _lib.OUTPUT_FIELDS])
         desc = self.desc(geometry, date, forcing.lfluxland)
         if accumulate:
             desc.flags |= _lib.SPD_ACCUMULATE_DIAGNOSTICS
         scratch = self._scratch_for(desc, dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        stream = current_raw_stream(didx)
         ev = C.c_void_p(marker.cuda_event) if marker is not None else None
         rc = lib.spd_fwd_marked(C.byref(desc), C.byref(geometry.vgrid()), C.byref(self._pstruct),
                                 C.byref(inp), C.byref(outs), _ptr(scratch), scratch.numel(),
