@@ -19,7 +19,8 @@
  *  - Return value 0 (SPD_OK) or one of the SPD_ERR_* codes; no exceptions cross the ABI.
  *  - The forward's output fields overlap neither its input fields nor one another
  *    (SPD_ERR_ALIAS): columns write their outputs while other columns still read their
- *    inputs, and its level-set launch reads the state before any output is written.
+ *    inputs, and a fixup launch (a missed level-set prediction) or the level-set launch
+ *    (SPD_NO_SPECULATION) reads the state again.
  */
 #ifndef SPEEDY_B200_H
 #define SPEEDY_B200_H

@@ -18,8 +18,10 @@
 // cloud-top level, the one cross-column dependency; column_second (radiation, surface fluxes,
 // vertical diffusion) needs the instance's level set of cloud tops and resumes from what the
 // first half left (qsat, the tendency accumulators, a few scalars).  The forward runs both in
-// one launch (speedy_kernels.cuh, fused_process) after a light launch that forms the level set
-// from column_first<KX, true>.
+// one launch (speedy_kernels.cuh, fused_process), with the level set predicted from the
+// previous call and checked by the launch's last block (a fixup launch redoes a missed
+// instance), or, under SPD_NO_SPECULATION, after a light launch that forms the level set from
+// column_first<KX, true>.
 //
 // Expression order follows the reference term by term (file:line relative to the JAX-GCM
 // root).  Deviations, all at the rounding level and never inside a cancelling difference:
