@@ -215,6 +215,14 @@ __device__ __forceinline__ ZonalRow zonal_row_of(const Derived& D, float sia, fl
 // first half, behind griddepcontrol.wait (when this launch overlaps the tail of a launch it
 // depends on, it waits there for that launch's completion; otherwise it returns at once).
 // Returns the column's own cloud-top level bit, 1 << clip(icltop, 0, kx-1).
+// The column's inputs are read with the streaming hint (ld.global.cs, evict first), as its
+// outputs are written (st.global.cs): each is touched once per call, and a call's hundreds of
+// megabytes would otherwise push the kernel's code, its constants and the per-latitude tables
+// out of L2 before the next call, whose first wave then fetched them from DRAM (measured with
+// per-block start and end times at T425: the first wave's blocks took 31.7 us against 23.6 us in
+// steady state, 25.2 us with the hint; the ensemble step went from 0.164 to 0.152 ms and the
+// T425 launch from 0.286 to 0.279 ms, results bitwise the same).
+// The level-set launch keeps the plain read-only path: the fused launch reads those rows again.
 template <int KX>
 __device__ __forceinline__ uint32_t fused_process(const ConstsD& CD, float* sm,
                                                   const spd_inputs_t& in,
@@ -228,15 +236,15 @@ __device__ __forceinline__ uint32_t fused_process(const ConstsD& CD, float* sm,
 #pragma unroll
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
-    t[k] = __ldg(in.temperature + i);
-    const float qk = __ldg(in.specific_humidity + i);
+    t[k] = __ldcs(in.temperature + i);
+    const float qk = __ldcs(in.specific_humidity + i);
     if (verify && qk < 0.0f) neg |= 1u << k;
     q[k] = (verify && qk < 0.0f) ? 0.0f : qk;
-    phi[k] = __ldg(in.geopotential + i);
+    phi[k] = __ldcs(in.geopotential + i);
   }
   SurfaceIn s;
-  s.psa = __ldg(in.normalized_surface_pressure + c);
-  s.fmask = __ldg(in.fmask + c);
+  s.psa = __ldcs(in.normalized_surface_pressure + c);
+  s.fmask = __ldcs(in.fmask + c);
   ColScalars o;
   {
     float qs[KX], dt[KX], dq[KX];
@@ -258,16 +266,16 @@ __device__ __forceinline__ uint32_t fused_process(const ConstsD& CD, float* sm,
     }
   }
   const size_t lw = low ? 0 : (size_t)(KX - 1) * C;
-  s.u_low = __ldg(in.u_wind + lw + c);
-  s.v_low = __ldg(in.v_wind + lw + c);
-  s.sst = __ldg(in.sea_surface_temperature + c);
-  s.stl = __ldg(in.stl_am + c);
-  s.soilw = __ldg(in.soilw_am + c);
-  s.snowc = __ldg(in.snowc_am + c);
-  s.sice = __ldg(in.sice_am + c);
-  s.alb0 = __ldg(in.alb0 + c);
-  s.orog = __ldg(in.orog + c);
-  s.phis0 = __ldg(in.phis0 + c);
+  s.u_low = __ldcs(in.u_wind + lw + c);
+  s.v_low = __ldcs(in.v_wind + lw + c);
+  s.sst = __ldcs(in.sea_surface_temperature + c);
+  s.stl = __ldcs(in.stl_am + c);
+  s.soilw = __ldcs(in.soilw_am + c);
+  s.snowc = __ldcs(in.snowc_am + c);
+  s.sice = __ldcs(in.sice_am + c);
+  s.alb0 = __ldcs(in.alb0 + c);
+  s.orog = __ldcs(in.orog + c);
+  s.phis0 = __ldcs(in.phis0 + c);
   const int j = c % il;
   const ZonalRow z = zonal_row_of(CD.D, __ldg(in.sia + j), __ldg(in.coa + j));
   asm volatile("griddepcontrol.wait;" ::: "memory");
