@@ -30,15 +30,15 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes (read + write) per column of the dominant kernel (ensemble_fused) and its warp
 # instructions per launch, from one ncu capture each (the summaries under profiles/ give the
-# commands): T425 from a --set full capture of one plain call (196.7 MB read + 171.1 MB
+# commands): T425 from a --set full capture of one plain call (196.8 MB read + 174.2 MB
 # written, 216.9 M warp instructions); the ensemble from the dram__bytes / inst_executed
-# metrics of one fused launch of the benchmark's step (96.2 MB read + 60.9 MB written, 103.8 M
+# metrics of one fused launch of the benchmark's step (96.2 MB read + 60.4 MB written, 103.8 M
 # warp instructions; one block per tile, the autotuner's pick); the adjoint (ensemble_adjoint, T170
 # with 16 levels) from a --set full capture of one VJP.  Part of each launch's writes is still
 # in L2 when the kernel ends, so the write share reads low.
-NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.210432e6 + 60.865024e6) / 466944,
-                          "t425": (196.710912e6 + 171.141376e6) / 819200}
-NCU_WARP_INSTRUCTIONS = {"ensemble": 103787429.0, "t425": 216853498.0,
+NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.215296e6 + 60.369920e6) / 466944,
+                          "t425": (196.767232e6 + 174.180096e6) / 819200}
+NCU_WARP_INSTRUCTIONS = {"ensemble": 103782785.0, "t425": 216850069.0,
                          "adjoint_t170": 117031373.0}
 
 
