@@ -152,6 +152,39 @@ def max_over_ranks(ms, dist, device):
     return float(t.item())
 
 
+def pcie_copy_ms(h2d, d2h, dev, reps=10):
+    """Time of one pinned host->device copy of h2d bytes and one device->host copy of d2h bytes
+    running at once on two streams (CUDA events, after three warm-up rounds)."""
+    import torch
+    h_up = torch.empty(h2d, dtype=torch.uint8, pin_memory=True)
+    h_dn = torch.empty(d2h, dtype=torch.uint8, pin_memory=True)
+    d_up = torch.empty(h2d, dtype=torch.uint8, device=dev)
+    d_dn = torch.empty(d2h, dtype=torch.uint8, device=dev)
+    s_up, s_dn = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    cur = torch.cuda.current_stream(dev)
+
+    def both():
+        s_up.wait_stream(cur)
+        s_dn.wait_stream(cur)
+        with torch.cuda.stream(s_up):
+            d_up.copy_(h_up, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            h_dn.copy_(d_dn, non_blocking=True)
+        cur.wait_stream(s_up)
+        cur.wait_stream(s_dn)
+
+    for _ in range(3):
+        both()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(cur)
+    for _ in range(reps):
+        both()
+    b.record(cur)
+    torch.cuda.synchronize(dev)
+    return a.elapsed_time(b) / reps
+
+
 def run_b200(args):
     import torch
     pkg = importlib.import_module("jax-gcm_b200")
@@ -400,9 +433,14 @@ def run_b200(args):
         e2e_ms = (timed(e2e_step, max(3, args.steps // 2), max(3, args.warmup)) /
                   max(3, args.steps // 2))
     if not args.no_e2e:
+        copy_ms = pcie_copy_ms(h2d, d2h, dev)
         e2e = {"value": cols * world / (e2e_ms / 1e3), "unit": "columns/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": round(e2e_ms, 4),
+               # the bus bound: the step's upload and download bytes alone, as one pinned copy
+               # each on two streams at once (no compute)
+               "pcie_copy_ms": round(copy_ms, 4),
+               "frac_of_pcie_copy": round(copy_ms / e2e_ms, 3),
                "path": ("batched.HostPipeline: one packed upload, spd_ensemble_fwd and one packed "
                         "download per step, consecutive steps overlapped" if ens is not None
                         else "per-member copies and spd_fwd calls")}
