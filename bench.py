@@ -664,14 +664,14 @@ def serving_section(pkg, dev, n_requests):
         warm.run([S.Request(S.TENDENCY, list(r.members)) for r in reqs[:8]] +
                  [S.Request(S.VJP, list(r.members)) for r in reqs[:2]])
         for label, stream in (("stream", reqs), ("saturation", sat)):
-            if label == "saturation":
-                # one unmeasured pass first: the first batches of a new size grow the pinned
-                # host cache and the device arena, a one-off cost of a server's warm-up
-                pre = S.Scheduler(be, src, budget, mode=mode)
-                pre.prefetch([k for r in stream for k in r.members])
-                pre.run([S.Request(r.kind, list(r.members), r.arrival, r.seed) for r in stream],
-                        timeout_s=600)
-                del pre
+            # one unmeasured pass first: the first batches of a new size grow the pinned host
+            # cache (a pinned allocation stalls the loop for milliseconds to tens of them) and
+            # the device arena, a one-off cost of a server's warm-up
+            pre = S.Scheduler(be, src, budget, mode=mode)
+            pre.prefetch([k for r in stream for k in r.members])
+            pre.run([S.Request(r.kind, list(r.members), r.arrival, r.seed) for r in stream],
+                    timeout_s=600)
+            del pre
             sch = S.Scheduler(be, src, budget, mode=mode)
             # member state is resident before traffic arrives (a resident-state service)
             sch.prefetch([k for r in stream for k in r.members])
