@@ -52,7 +52,7 @@ def test_library_rejects_overlapping_outputs():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kx,ix,il", [(8, 96, 48), (16, 128, 64), (16, 7, 5)])
+@pytest.mark.parametrize("kx,ix,il", [(8, 96, 48), (16, 128, 64), (16, 7, 5), (7, 64, 32)])
 def test_gpu_matches_oracle(kx, ix, il):
     import torch
     inst = _state(40 + kx + ix, kx, ix, il)
