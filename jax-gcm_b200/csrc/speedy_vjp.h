@@ -234,8 +234,13 @@ SPD_HD void dconv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c,
   const F qthr0 = g.rhbl * c.qsat[KX - 1];
   if (c.case1) {
     const F mse0 = c.SE(KX - 1) + F(2501.0) * c.q[KX - 1];
-    const int j = c.ktop2 - 1;
-    const F msthr = mss2_at(x, c, j);
+    // the threshold level j = ktop2 - 1, matched in a loop so that the per-level arrays are
+    // addressed by constants
+    const int jt = c.ktop2 - 1;
+    F msthr = F(0);
+    SPD_LEVELS
+    for (int j = 0; j < KX; ++j)
+      if (j == jt) msthr = mss2_at(x, c, j);
     const F A = c.q[KX - 1] - qthr0;
     const F B = (mse0 - msthr) * F(1.0 / 2501.0);
     const F Ab = qdif_b * wmax(A, B);
@@ -246,7 +251,9 @@ SPD_HD void dconv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c,
     const F msthr_b = -mse0_b;
     b.add_se(KX - 1, mse0_b);
     b.q[KX - 1] += F(2501.0) * mse0_b;
-    if (j < KX - 1) {
+    SPD_LEVELS
+    for (int j = 0; j < KX - 1; ++j) {
+      if (j != jt) continue;
       const F w = F(x.vg->wvi[j][1]);
       const F m0b = msthr_b - w * msthr_b, m1b = w * msthr_b;
       b.add_se(j, m0b);
@@ -347,13 +354,17 @@ SPD_HD void conv(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<K
   w.dfqa[KX - 1] = w.dfqa[KX - 1] + (-fsq_sum);
   w.precnv = F(0);
   w.qsatb = w.X = F(0);
-  if (iptop <= KX - 1) {
-    const int kt = iptop - 1;
+  // the top layer k = iptop (1 <= iptop <= kx - 1): a loop over the levels with one match
+  // instead of an index, so that the per-level arrays are addressed by constants
+  SPD_LEVELS
+  for (int k = 1; k < KX; ++k) {
+    if (k != iptop) continue;
+    const int kt = k - 1;
     w.qsatb = c.qsat[kt] + F(vg.wvi[kt][1]) * (c.qsat[kt + 1] - c.qsat[kt]);
-    w.X = w.fuq3[iptop] - w.fm3[iptop] * w.qsatb;
+    w.X = w.fuq3[k] - w.fm3[k] * w.qsatb;
     w.precnv = vmax(w.X, F(0));
-    w.dfse[kt] = w.fus3[iptop] - w.fds3[iptop] + F(2501.0) * w.precnv;
-    w.dfqa[kt] = w.fuq3[iptop] - w.fdq3[iptop] - w.precnv;
+    w.dfse[kt] = w.fus3[k] - w.fds3[k] + F(2501.0) * w.precnv;
+    w.dfqa[kt] = w.fuq3[k] - w.fdq3[k] - w.precnv;
   }
   w.rps = F(1) / c.psa;
 }
@@ -389,19 +400,21 @@ SPD_HD F conv_rev(const Ctx& x, const DiffParams<F>& g, const Col<KX, F>& c, Cv<
   SPD_LEVELS
   for (int k = 0; k < KX; ++k)
     fus3_b[k] = fuq3_b[k] = fds3_b[k] = fdq3_b[k] = fm3_b[k] = sb3_b[k] = qb3_b[k] = F(0);
-  if (iptop <= KX - 1) {
-    const int kt = iptop - 1;
+  SPD_LEVELS
+  for (int k = 1; k < KX; ++k) {  // the top layer k = iptop, addressed by constants
+    if (k != iptop) continue;
+    const int kt = k - 1;
     const F se_b = dfse_b[kt], qa_b = dfqa_b[kt];
-    fus3_b[iptop] += se_b;
-    fds3_b[iptop] -= se_b;
-    fuq3_b[iptop] += qa_b;
-    fdq3_b[iptop] -= qa_b;
+    fus3_b[k] += se_b;
+    fds3_b[k] -= se_b;
+    fuq3_b[k] += qa_b;
+    fdq3_b[k] -= qa_b;
     const F pb = precnv_b + F(2501.0) * se_b - qa_b;
     dfse_b[kt] = dfqa_b[kt] = F(0);
     const F Xb = pb * wmax(w.X, F(0));
-    fuq3_b[iptop] += Xb;
-    fm3_b[iptop] -= Xb * w.qsatb;
-    const F qsatb_b = -Xb * w.fm3[iptop];
+    fuq3_b[k] += Xb;
+    fm3_b[k] -= Xb * w.qsatb;
+    const F qsatb_b = -Xb * w.fm3[k];
     const F ww = F(vg.wvi[kt][1]);
     b.qsat[kt] += qsatb_b - ww * qsatb_b;
     b.qsat[kt + 1] += ww * qsatb_b;
