@@ -32,10 +32,16 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 # instruction issue, IEEE division and subnormal handling cost several instructions each, and
 # measured against the oracles they change nothing (tendencies, precipitation and diagnostics
 # keep their distances at the printed digits; the only values flushed are transmissivities below
-# 1e-38).  The adjoint keeps IEEE arithmetic.
+# 1e-38).  The adjoint keeps IEEE division and subnormals and is compiled without contraction
+# too: its kernel exists in two register budgets (four or two blocks per SM, chosen by the
+# batch's tile count), and only separately rounded arithmetic makes the two give the same bits,
+# so that a member's gradients do not depend on the batch it is served in (with contraction
+# ptxas fused different products in the two; without it the T170 VJP takes 0.566 against
+# 0.529 ms, and the reference's float32 arithmetic rounds every operation as well).
 FORWARD_FLAGS = ["-fmad=false", "-prec-div=false", "-ftz=true"]
 SOURCE_FLAGS = {"csrc/speedy_ensemble.cu": FORWARD_FLAGS,
-                "csrc/speedy_selftest.cu": FORWARD_FLAGS}  # checks the forward's arithmetic
+                "csrc/speedy_selftest.cu": FORWARD_FLAGS,  # checks the forward's arithmetic
+                "csrc/speedy_adjoint.cu": ["-fmad=false"]}
 
 
 def _nvcc():

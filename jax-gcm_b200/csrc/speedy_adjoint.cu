@@ -47,7 +47,7 @@ __device__ __forceinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t&
   g.drhlsc = A.p.drhlsc; g.rhblsc = A.p.rhblsc; g.albcl = A.p.albcl; g.albcls = A.p.albcls;
   spdgen::ColumnIn<float, float> xi;
   float ct_t[KX], ct_q[KX];
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
     xi.t[k] = __ldg(in.temperature + i);
@@ -76,7 +76,7 @@ __device__ __forceinline__ void vjp_column(const VjpArgs& A, const spd_inputs_t&
   spdvjp::column_vjp<KX, float>(x, g, A.ablco2, A.dt_seconds, A.q_tend_scale, xi, ct_t, ct_q,
                                 __ldg(ct.u_wind + lo), __ldg(ct.v_wind + lo), b, A.qcorv,
                                 A.gamlat, A.pexp);
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < KX; ++k) {
     const size_t i = (size_t)k * C + c;
     gr.temperature[i] = b.t[k];
@@ -137,7 +137,15 @@ __global__ void __launch_bounds__(kBlock)
   prepass_tiles(A, members, tiles, ntiles);
 }
 
-__global__ void __launch_bounds__(kAdjBlock, 4)
+// Two register budgets of the same kernel: 128 registers for four blocks per SM, or 255 for two
+// (1,376 against 2,088 bytes of stack, ptxas).  Two blocks per SM is the faster where every
+// tile of the batch is resident at once (T85 with 16 levels, 256 tiles: 0.134 against
+// 0.194 ms); four is the faster at T170 (1,024 tiles, 1.73 waves of four-per-SM residency
+// against 3.46 of two).  The launch takes two per SM when the tiles fit in one such wave.  The
+// translation unit is compiled without multiply-add contraction, so the two give the same bits
+// (a member's gradients do not depend on the batch that carried it).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kAdjBlock, kMinBlocks)
     ensemble_adjoint(const __grid_constant__ VjpClassArgs A,
                      const VjpMemberDev* __restrict__ members, const Tile* __restrict__ tiles,
                      int ntiles) {
@@ -184,7 +192,8 @@ int preload_adjoint() {
   bool ok = true;
   ok &= cudaFuncGetAttributes(&a, vjp_single_plan) == cudaSuccess;
   ok &= cudaFuncGetAttributes(&a, ensemble_vjp_prepass) == cudaSuccess;
-  ok &= cudaFuncGetAttributes(&a, ensemble_adjoint) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_adjoint<4>) == cudaSuccess;
+  ok &= cudaFuncGetAttributes(&a, ensemble_adjoint<2>) == cudaSuccess;
   return ok ? SPD_OK : SPD_ERR_CUDA;
 }
 
@@ -202,8 +211,15 @@ static int launch_ensemble_vjp(const ClassArgs& P, const VjpClassArgs& V, char* 
   const int grid_pre = std::min(ntiles, 65535);
   if (cudaMemsetAsync(base + levelset_offset, 0, levelset_bytes, st) != cudaSuccess)
     return SPD_ERR_CUDA;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return SPD_ERR_CUDA;
   ensemble_vjp_prepass<<<grid_pre, kBlock, 0, st>>>(P, md, tl, ntiles);
-  ensemble_adjoint<<<grid, kAdjBlock, 0, st>>>(V, md, tl, ntiles);
+  if (grid <= 2 * sms)
+    ensemble_adjoint<2><<<grid, kAdjBlock, 0, st>>>(V, md, tl, ntiles);
+  else
+    ensemble_adjoint<4><<<grid, kAdjBlock, 0, st>>>(V, md, tl, ntiles);
   return cudaGetLastError() == cudaSuccess ? SPD_OK : SPD_ERR_CUDA;
 }
 
