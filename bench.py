@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 NCU_TRAFFIC_PER_COLUMN = {"ensemble": (96.215296e6 + 60.369920e6) / 466944,
                           "t425": (196.767232e6 + 174.180096e6) / 819200}
 NCU_WARP_INSTRUCTIONS = {"ensemble": 103782785.0, "t425": 216850069.0,
-                         "adjoint_t170": 117031373.0}
+                         "adjoint_t170": 129642118.0}
 
 
 def parse_args():
