@@ -259,6 +259,10 @@ int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_l
     pf_lvl = grid_lvl;
   }
   const size_t arena = arena_bytes(kx_layout);
+  // the fixup is one resident wave striding over the tiles: its blocks read one word and return
+  // when no prediction missed, and a grid of one block per tile spends microseconds on
+  // scheduling thousands of such blocks
+  const int grid_fix = std::min(grid_cols, res_cols);
   // the launch words and every member's T and R start at zero; P is kept from the last call
   if (cudaMemsetAsync(T.launch, 0, clear_bytes, st) != cudaSuccess) return SPD_ERR_CUDA;
   int r;
@@ -266,10 +270,10 @@ int launch_forward(const ClassArgs& A, const TileSource& T, int ntiles, int kx_l
     ensemble_fused<<<grid_cols, kNT, arena, st>>>(A, T, ntiles, 1);
     if (marker) {  // timing hook: the fused launch apart, then the fixup in plain stream order
       if (cudaEventRecord(marker, st) != cudaSuccess) return SPD_ERR_CUDA;
-      ensemble_fixup<<<grid_cols, kNT, arena, st>>>(A, T, ntiles);
+      ensemble_fixup<<<grid_fix, kNT, arena, st>>>(A, T, ntiles);
       r = SPD_OK;
     } else {
-      r = launch_dependent(ensemble_fixup, grid_cols, arena, st, A, T, ntiles);
+      r = launch_dependent(ensemble_fixup, grid_fix, arena, st, A, T, ntiles);
     }
   } else {
     ensemble_levelset<<<grid_lvl, kNT, 0, st>>>(A, T, ntiles, pf_lvl);
