@@ -82,3 +82,21 @@ def test_ensemble_prediction_misses_only_on_the_first_call(pkg):
     for o, r in zip([m.out for m in ens.members], ref):
         for k in r:
             assert torch.equal(o[k], r[k]), k
+
+
+def test_large_instance_redo_strides_over_the_tiles(pkg):
+    """A 1024-tile instance (more tiles than the GPU holds blocks at once): its first call
+    misses, and the fixup launch -- one resident wave of blocks striding over the tiles --
+    redoes every tile; a second call hits.  Both equal the non-speculating forward bitwise."""
+    inst = pkg.synthetic.land_instance(77, 512, 256, 16)
+    ref = run_gpu_instance(pkg, inst, speculate=False)
+    phys = pkg.SpeedyPhysics(speculate=True)
+    st, fo, ge, da = to_device(pkg, inst, "cuda")
+    for call in range(2):
+        tend, data = phys.compute_tendencies(st, fo, ge, da)
+        torch.cuda.synchronize()
+        got = dict(u_wind=tend.u_wind, v_wind=tend.v_wind, temperature=tend.temperature,
+                   specific_humidity=tend.specific_humidity, precnv=data.convection.precnv,
+                   precls=data.condensation.precls)
+        for k in FIELDS:
+            assert np.array_equal(got[k].cpu().numpy(), ref[k]), (call, k)
