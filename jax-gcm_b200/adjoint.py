@@ -18,7 +18,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .physics import (Parameters, PhysicsState, PhysicsTendency, SpeedyPhysics)
+from .physics import (Parameters, PhysicsState, PhysicsTendency, SpeedyPhysics,
+                      current_raw_stream)
 
 DIFF_PARAMS = [("convection", "psmin"), ("convection", "trcnv"), ("convection", "rhil"),
                ("convection", "rhbl"), ("convection", "entmax"), ("convection", "smf"),
@@ -47,10 +48,14 @@ def _input_struct(state, forcing, geometry):
              sea_surface_temperature=f2.sea_surface_temperature, fmask=geometry.fmask,
              orog=geometry.orog, phis0=geometry.phis0, sia=geometry.sia, coa=geometry.coa)
     dev = state.temperature.device
-    for k, v in t.items():
-        if v.dtype != torch.float32 or not v.is_contiguous() or v.device != dev:
-            t[k] = v.to(device=dev, dtype=torch.float32).contiguous()
-    return _lib.Inputs(**{k: t[k].data_ptr() for k in _lib.INPUT_FIELDS}), t
+    didx = state.temperature.get_device()
+    ptrs = []
+    for k in _lib.INPUT_FIELDS:
+        v = t[k]
+        if v.dtype is not torch.float32 or not v.is_contiguous() or v.get_device() != didx:
+            v = t[k] = v.to(device=dev, dtype=torch.float32).contiguous()
+        ptrs.append(v.data_ptr())
+    return _lib.Inputs(*ptrs), t
 
 
 def vjp(physics: SpeedyPhysics, state: PhysicsState, forcing, geometry, date,
@@ -73,7 +78,7 @@ def vjp(physics: SpeedyPhysics, state: PhysicsState, forcing, geometry, date,
     desc = physics.desc(geometry, date, forcing.lfluxland)
     n = lib.spd_vjp_scratch_bytes(C.byref(desc))
     sc = _scratch(n, dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
+    stream = current_raw_stream(state.temperature.get_device())
     rc = lib.spd_vjp(C.byref(desc), C.byref(geometry.vgrid()), C.byref(physics._pstruct),
                      C.byref(inp), C.byref(cts), C.byref(grads), C.c_void_p(sc.data_ptr()), n,
                      C.c_void_p(stream))
