@@ -4,12 +4,21 @@
 // A member is one grid instance (its own arrays, ix*il columns, kx levels).  The plan splits
 // every member into tiles of kNT consecutive columns (a tile never straddles members), ordered
 // by level count (16-level tiles first, the heavier work), and keeps per member the field
-// pointers, its cloud-top level-set word and its per-latitude solar table.  Launch 1 (light)
-// forms each member's level set S and solar table from the cloud-top part of every column;
-// launch 2 runs every column whole, in one pass, reading its member's S (the one cross-column
-// dependency, shortwave_radiation.py:62-68) and solar table.  Both launches are persistent:
-// gridDim blocks stride over the tile list.  The plain per-instance forward (spd_fwd) runs the
-// same two kernels over a one-member plan given by value, so that the two paths agree bitwise.
+// pointers and its cloud-top level-set words (P: the prediction, T: the true set, R: missed).
+// The one cross-column dependency is the level set S (shortwave_radiation.py:62-68).  Two
+// launch forms:
+//   speculating (the default): the fused launch runs every column whole, in one pass, with
+//     each member's predicted set P (the previous call's) while the columns OR their own cloud
+//     tops into T; its last block compares T with P and marks the members that missed (R).
+//     The fixup launch, a programmatic dependent launch of one resident wave, computes the
+//     missed members again with their true set; when none missed its blocks read one word
+//     and return.
+//   level set first (accumulating calls, which must not add a column's diagnostics twice, and
+//     calls that ask for no prediction): a light launch forms every member's S from the
+//     cloud-top part of every column, then the fused launch reads it.
+// The launches are persistent or one block per tile (gridDim blocks stride over the tile
+// list).  The plain per-instance forward (spd_fwd) runs the same kernels over a one-member
+// plan given by value, so that the two paths agree bitwise.
 // Constants shared by a class of members (kx, date, switches, vertical grid, parameters) travel
 // by value in the kernel parameters.
 #include <cuda_runtime.h>
