@@ -683,6 +683,9 @@ def serving_section(pkg, dev, n_requests):
             st["uploads_during_run"] = sch.stats.get("uploads", 0)
             st["prefetched_members"] = sch.stats.get("prefetched", 0)
             st["peak_budget_bytes"] = sch.peak
+            # the loop's passes over 5 ms (wall, CPU and context switches), longest first
+            st["slow_passes"] = len(sch.slow_passes)
+            st["slowest_passes"] = sorted(sch.slow_passes, key=lambda p: -p["wall_ms"])[:4]
             out[f"{mode}_{label}"] = {k: (round(v, 3) if isinstance(v, float) else v)
                                       for k, v in st.items()}
             del sch, fin

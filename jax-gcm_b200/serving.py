@@ -8,8 +8,8 @@ layer a forecast service would put in front of the physics:
 
 * Admission by free HBM.  Every device byte the loop holds (resident member state, result and
   cotangent buffers, the adjoint's scratch) is counted against ``budget_bytes``, and a request
-  must also fit the device memory the backend can still hand out (its pool's free bytes plus
-  the driver's free memory, measured at admission).  A request is admitted, in arrival order,
+  must also fit the device memory the backend can still hand out (its pool's free bytes, plus
+  the driver's free memory when the pool would have to grow).  A request is admitted, in arrival order,
   when its new members and its result buffers fit; idle resident members are evicted
   least-recently-used to make room.  A request that can never fit is
   rejected; a failed device allocation leaves the request waiting and is counted.
@@ -40,6 +40,7 @@ from __future__ import annotations
 import collections
 import ctypes as C
 import gc
+import resource
 import time
 from dataclasses import dataclass, field
 from typing import Callable, Dict, Hashable, List, Optional
@@ -178,12 +179,20 @@ class Scheduler:
 
     ``freeze_gc`` (default on) keeps the garbage collector's full collections off the loop
     during ``run``; a caller that drives ``step`` itself can do the same with ``gc.freeze``.
+
+    ``slow_passes`` (filled by ``run``): every pass of the loop that took longer than
+    ``slow_pass_ms`` of wall time, with the time spent in submission, ``poll``, ``admit`` and
+    ``launch``, the loop thread's CPU time over the pass and its voluntary and involuntary
+    context switches (a pass whose CPU time is far below its wall time, with involuntary
+    switches, was descheduled by the operating system; one with voluntary switches waited in
+    a blocking call).
     """
 
     def __init__(self, backend, source: Callable[[Hashable], HostMember], budget_bytes: int,
                  mode: str = "batched", max_inflight: int = 2, max_batch_columns: int = 1 << 24,
                  on_complete: Optional[Callable[[Request], None]] = None,
-                 max_admit_per_step: int = 8, freeze_gc: bool = True):
+                 max_admit_per_step: int = 8, freeze_gc: bool = True,
+                 slow_pass_ms: float = 5.0):
         if mode not in ("batched", "plain"):
             raise ValueError("mode is 'batched' or 'plain'")
         self.b = backend
@@ -210,6 +219,9 @@ class Scheduler:
         self._rid = 0
         self._tick = 0
         self.stats = collections.Counter()
+        self.slow_pass_ms = float(slow_pass_ms)
+        self.slow_passes: List[dict] = []
+        self._phase = (0.0, 0.0, 0.0)
 
     # -- submission -----------------------------------------------------------------------------
     def _host(self, key):
@@ -282,7 +294,7 @@ class Scheduler:
         if self.budget - self.used < nbytes:
             return False
         avail = getattr(self.b, "available_bytes", None)
-        return avail is None or avail() >= nbytes
+        return avail is None or avail(nbytes) >= nbytes
 
     def _evict_for(self, nbytes, keep):
         idle = sorted((r for r in self.resident.values() if r.refs == 0 and r.key not in keep),
@@ -441,7 +453,14 @@ class Scheduler:
 
     def step(self):
         """One pass of the loop: retire, admit, launch.  Returns the amount of work done."""
-        return self.poll() + self.admit() + self.launch()
+        t0 = time.perf_counter()
+        a = self.poll()
+        t1 = time.perf_counter()
+        b = self.admit()
+        t2 = time.perf_counter()
+        c = self.launch()
+        self._phase = (t1 - t0, t2 - t1, time.perf_counter() - t2)
+        return a + b + c
 
     def run(self, requests: List[Request], timeout_s: float = 600.0):
         """Serve ``requests`` (their ``arrival`` times in seconds after the start) in real time
@@ -461,11 +480,18 @@ class Scheduler:
         try:
             self.b.start_clock()
             t_end = time.perf_counter() + timeout_s
+            wall, cpu, sw = time.perf_counter(), time.thread_time(), _switches()
             while pending or self.busy():
                 now = self.b.now()
                 while pending and pending[0].arrival <= now:
                     self.submit(pending.popleft())
-                if self.step() == 0 and time.perf_counter() > t_end:
+                t_sub = time.perf_counter()
+                idle = self.step() == 0
+                w1 = time.perf_counter()
+                if (w1 - wall) * 1e3 > self.slow_pass_ms:
+                    self._slow_pass(now, wall, cpu, sw, t_sub, w1)
+                wall, cpu, sw = w1, time.thread_time(), _switches()
+                if idle and w1 > t_end:
                     raise TimeoutError(f"serving loop exceeded {timeout_s} s "
                                        f"({len(pending)} pending, {len(self.inflight)} in flight)")
             self.b.synchronize()
@@ -473,6 +499,25 @@ class Scheduler:
             if self.freeze_gc:
                 gc.unfreeze()
         return self.finished
+
+    def _slow_pass(self, now, wall, cpu, sw, t_sub, w1):
+        sw1 = _switches()
+        poll, admit, launch = self._phase
+        self.slow_passes.append(dict(
+            at_s=round(now, 4), wall_ms=round((w1 - wall) * 1e3, 3),
+            cpu_ms=round((time.thread_time() - cpu) * 1e3, 3),
+            submit_ms=round((t_sub - wall) * 1e3, 3), poll_ms=round(poll * 1e3, 3),
+            admit_ms=round(admit * 1e3, 3), launch_ms=round(launch * 1e3, 3),
+            voluntary=sw1[0] - sw[0], involuntary=sw1[1] - sw[1]))
+
+
+def _switches():
+    """(voluntary, involuntary) context switches of the calling thread so far."""
+    try:
+        r = resource.getrusage(resource.RUSAGE_THREAD)
+    except (AttributeError, OSError):
+        return (0, 0)
+    return (r.ru_nvcsw, r.ru_nivcsw)
 
 
 def latency_stats(finished: List[Request]):
@@ -787,18 +832,23 @@ class CudaBackend:
         dm.handle = handle
         return dm
 
-    def available_bytes(self):
+    def available_bytes(self, need=None):
         """Device bytes this backend can still hand out: its pool's free bytes, plus the
         device's free memory (the pool grows into it), less a 1 GiB margin for the driver and
-        other users of the device.  The driver's figure is measured at most every half second
-        and after the pool grows (cudaMemGetInfo on every admission cost the request loop
-        milliseconds per request), the pool's own figure exactly."""
+        other users of the device.  When the pool's own free bytes cover ``need`` that figure
+        is returned as it is: the driver's free memory (cudaMemGetInfo) is asked for only when
+        the pool may have to grow, because the query waits on the device -- in the request
+        loop it blocked a pass for 6-16 ms while batches ran.  The driver's figure is measured
+        at most every half second and after the pool grows, the pool's own figure exactly."""
+        pool_free = self.arena.reserved - self.arena.in_use
+        if need is not None and pool_free >= need:
+            return pool_free
         now = time.perf_counter()
         if (self._free_at is None or now - self._free_at > 0.5 or
                 self._free_reserved != self.arena.reserved):
             self._dev_free = int(self.torch.cuda.mem_get_info(self.dev)[0])
             self._free_at, self._free_reserved = now, self.arena.reserved
-        return (self.arena.reserved - self.arena.in_use) + max(0, self._dev_free - (1 << 30))
+        return pool_free + max(0, self._dev_free - (1 << 30))
 
     def release(self, dm):
         # The member's upload may still be running on the copy stream (a prefetched member, or

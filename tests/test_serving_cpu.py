@@ -275,6 +275,30 @@ def test_run_loop_real_time_with_fake_device():
     assert all(r.t_done >= r.arrival for r in fin)
 
 
+def test_slow_passes_name_the_phase_and_the_wait():
+    """A launch that blocks for 30 ms shows as one slow pass: its time in launch, little
+    CPU time, and a voluntary context switch (a blocking wait, not a preemption)."""
+    import time
+    src, _ = make_source(a=(8, 64, 32))
+    blocked = []
+
+    class Blocking(FakeBackend):
+        def launch(self, kind, reqs, devs):
+            if not blocked:
+                blocked.append(True)
+                time.sleep(0.03)
+            return super().launch(kind, reqs, devs)
+
+    sch = S.Scheduler(Blocking(per_col=1e-8, realtime=True), src, 1 << 30, slow_pass_ms=20.0)
+    sch.run([S.Request(S.TENDENCY, ["a"], arrival=0.001 * i) for i in range(4)], timeout_s=30)
+    assert len(sch.slow_passes) >= 1
+    p = max(sch.slow_passes, key=lambda p: p["wall_ms"])
+    assert p["wall_ms"] >= 29.0 and p["launch_ms"] >= 29.0
+    assert p["cpu_ms"] < 0.5 * p["wall_ms"]
+    assert p["voluntary"] >= 1
+    assert set(p) >= {"at_s", "submit_ms", "poll_ms", "admit_ms", "involuntary"}
+
+
 def test_run_freezes_the_collector_for_its_duration():
     import gc
     src, _ = make_source(a=(8, 64, 32))
@@ -419,6 +443,33 @@ def test_cuda_backend_release_waits_for_the_upload_before_freeing():
     assert dm.buf is None
 
 
+def test_cuda_backend_asks_the_driver_only_when_the_pool_may_grow():
+    """CudaBackend.available_bytes answers from its pool while the pool's free bytes cover the
+    request; the driver's free memory (a query that waits on the device) is asked for only
+    when they do not.  No device is touched (the arena and torch are fakes)."""
+    S = pkg.serving
+    asked = []
+
+    class Cuda:
+        @staticmethod
+        def mem_get_info(dev):
+            asked.append(dev)
+            return (10 << 30, 80 << 30)
+
+    class Torch:
+        cuda = Cuda
+
+    class Arena:
+        reserved, in_use = 4 << 30, 1 << 30
+
+    be = S.CudaBackend.__new__(S.CudaBackend)
+    be.arena, be.torch, be.dev = Arena(), Torch(), 0
+    be._free_at, be._free_reserved, be._dev_free = None, None, 0
+    assert be.available_bytes(2 << 30) == 3 << 30 and asked == []
+    assert be.available_bytes(5 << 30) == (3 << 30) + (9 << 30) and asked == [0]
+    assert be.available_bytes() == (3 << 30) + (9 << 30) and asked == [0]   # half-second cache
+
+
 def test_admission_waits_for_free_device_memory_below_the_budget():
     """A backend that measures its free device memory below what the budget would allow:
     requests are admitted only as far as that memory goes (idle members evicted first), the
@@ -429,7 +480,7 @@ def test_admission_waits_for_free_device_memory_below_the_budget():
             self.limit = limit
             self.held = {}
 
-        def available_bytes(self):
+        def available_bytes(self, need=None):
             return self.limit - sum(self.held.values())
 
         def upload(self, h):
